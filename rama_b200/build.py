@@ -1,0 +1,71 @@
+"""Builds the in-tree native artefacts for sm_100a.
+
+    python -m rama_b200.build [--force]
+
+* rama_b200/librama_b200.so   -- the CUDA solver behind include/rama_b200.h
+* rama_b200/bin/rama_text_input -- the command-line front end
+
+A target is rebuilt when any of its sources is newer than it.
+"""
+from __future__ import annotations
+
+import glob
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+INCLUDE = os.path.join(ROOT, "include")
+LIB = os.path.join(HERE, "librama_b200.so")
+CLI = os.path.join(HERE, "bin", "rama_text_input")
+NVCC = os.environ.get("NVCC", "nvcc")
+
+NVCC_FLAGS = [
+    "-gencode", "arch=compute_100a,code=sm_100a",
+    "-std=c++17", "-O3", "-lineinfo",
+    # strict IEEE arithmetic so that results match the CPU oracle bit for bit
+    "-fmad=false",
+    "--expt-relaxed-constexpr", "--extended-lambda",
+    "-Xcompiler", "-fPIC",
+]
+
+
+def _stale(target, sources):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(s) > t for s in sources)
+
+
+def build_lib(force=False, verbose=False):
+    srcs = glob.glob(os.path.join(HERE, "csrc", "*")) + [os.path.join(INCLUDE, "rama_b200.h")]
+    if not force and not _stale(LIB, srcs):
+        return LIB
+    cmd = [NVCC, *NVCC_FLAGS, "-shared", "-o", LIB + ".tmp", os.path.join(HERE, "csrc", "capi.cu")]
+    if verbose:
+        cmd.insert(1, "-Xptxas=-v")
+    subprocess.run(cmd, check=True)
+    os.replace(LIB + ".tmp", LIB)
+    return LIB
+
+
+def build_cli(force=False):
+    src = os.path.join(HERE, "cli", "rama_text_input.cpp")
+    hdrs = glob.glob(os.path.join(INCLUDE, "*.h"))
+    if not force and not _stale(CLI, [src, LIB, *hdrs]):
+        return CLI
+    os.makedirs(os.path.dirname(CLI), exist_ok=True)
+    subprocess.run(["g++", "-std=c++17", "-O2", "-I", INCLUDE, "-o", CLI, src, "-L", HERE, "-l:librama_b200.so",
+                    "-Wl,-rpath,$ORIGIN/.."], check=True)
+    return CLI
+
+
+def build(force=False):
+    build_lib(force)
+    build_cli(force)
+
+
+if __name__ == "__main__":
+    build(force="--force" in sys.argv)
+    print("built", LIB, "and", CLI)

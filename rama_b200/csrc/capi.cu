@@ -1,0 +1,757 @@
+// capi.cu -- kernels and the C ABI of librama_b200.so (include/rama_b200.h).
+//
+// Two kernels run the same device solver (solver.cuh):
+//   k_solve_cta  : persistent CTAs; each pulls instances from a queue (largest
+//                  first) and solves them alone (BlockTeam).  Used for batches
+//                  and for small single instances.
+//   k_solve_grid : one cooperative launch; the whole GPU solves one instance
+//                  (GridTeam).
+// Both take their scratch memory from a workspace the handle owns.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "../../include/rama_b200.h"
+#include "solver.cuh"
+
+using namespace rama;
+
+namespace {
+
+constexpr int THREADS = 512;
+constexpr int SMEM = sort_smem_bytes(THREADS) + 1024;
+constexpr uint64_t PART_BYTES = 16 * 4096;  // >= 16 * (max CTAs + 2)
+constexpr int64_t BLOCK_TEAM_MAX_EDGES = 200000;
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string &msg)
+{
+    g_err = msg;
+    return code;
+}
+
+#define CU(call)                                                                               \
+    do {                                                                                       \
+        cudaError_t e_ = (call);                                                               \
+        if (e_ != cudaSuccess) return fail(RAMA_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+__device__ __forceinline__ Scratch make_scratch(char *base, uint64_t bytes)
+{
+    Scratch sc;
+    sc.part[0] = base;
+    sc.part[1] = base + PART_BYTES;
+    sc.parity = 0;
+    sc.arena.base = base;
+    sc.arena.cap = bytes - 256;
+    sc.arena.lo = 2 * PART_BYTES;
+    sc.arena.top = sc.arena.cap;
+    sc.arena.peak = sc.arena.lo;
+    sc.arena.failed = 0;
+    return sc;
+}
+
+struct CtaLaunch {
+    Options opts;
+    Instance *inst;
+    const int32_t *order;
+    int32_t count;
+    int32_t *queue;
+    char *ws;
+    uint64_t ws_per_cta;
+};
+
+__global__ void __launch_bounds__(THREADS, 2) k_solve_cta(CtaLaunch L)
+{
+    extern __shared__ __align__(16) char sm[];
+    __shared__ int next;
+    BlockTeam t;
+    char *base = L.ws + (uint64_t)blockIdx.x * L.ws_per_cta;
+    for (int guard = 0; guard < (1 << 30); ++guard) {
+        if (threadIdx.x == 0) next = atomicAdd(L.queue, 1);
+        __syncthreads();
+        const int k = next;
+        __syncthreads();
+        if (k >= L.count) break;
+        Scratch sc = make_scratch(base, L.ws_per_cta);
+        solve_instance(t, sm, sc, L.opts, &L.inst[L.order[k]]);
+        __syncthreads();
+    }
+}
+
+struct GridLaunch {
+    Options opts;
+    Instance *inst;
+    char *ws;
+    uint64_t ws_bytes;
+};
+
+__global__ void __launch_bounds__(THREADS, 2) k_solve_grid(GridLaunch L)
+{
+    extern __shared__ __align__(16) char sm[];
+    GridTeam t;
+    Scratch sc = make_scratch(L.ws, L.ws_bytes);
+    solve_instance(t, sm, sc, L.opts, L.inst);
+}
+
+// ---------------------------------------------------------------------------
+// single steps
+// ---------------------------------------------------------------------------
+template <class Team>
+__device__ void copy_graph_out(const Team &t, const Graph &g, rama_step_args *a)
+{
+    if (g.n <= a->out_cap)
+        for (int64_t e = t.rank(); e < g.n; e += t.size()) {
+            a->out_row[e] = g.row[e];
+            a->out_col[e] = g.col[e];
+            a->out_cost[e] = g.cost[e];
+        }
+    if (t.leader()) {
+        a->out_n = g.n;
+        a->out_rows = g.rows;
+        a->out_cols = g.cols;
+        if (g.n > a->out_cap) a->status |= ERR_INVALID_ARG;
+    }
+}
+
+template <class Team>
+__device__ void run_step(const Team &t, char *sm, Scratch sc, rama_step_args *a)
+{
+    Graph A;
+    A.row = const_cast<int32_t *>(a->row);
+    A.col = const_cast<int32_t *>(a->col);
+    A.cost = const_cast<float *>(a->cost);
+    A.n = a->n;
+    A.rows = a->rows;
+    A.cols = a->cols;
+    const int op = a->op;
+    if (op == RAMA_STEP_INIT) {
+        Graph g = graph_from_edges(t, sc, sm, a->i, a->j, a->c, a->m);
+        if (sc.arena.ok()) copy_graph_out(t, g, a);
+    } else if (op == RAMA_STEP_CONTRACT) {
+        int32_t mx = team_max<Team, int32_t>(t, sc, sm, a->map_size, 0, [&](int64_t k) { return a->map[k]; });
+        Graph g = graph_contract_raw(t, sc, sm, A, a->map, mx);
+        if (sc.arena.ok()) copy_graph_out(t, g, a);
+    } else if (op == RAMA_STEP_MATCHING) {
+        int32_t M = 0;
+        int32_t nr = matching_contraction_map(t, sc, sm, A, a->mean_multiplier_mm, a->out_map, &M);
+        if (t.leader()) {
+            a->out_nr = nr;
+            a->out_count = M;
+        }
+    } else if (op == RAMA_STEP_WOC) {
+        int32_t sz = 0;
+        int err = 0;
+        int32_t nr = woc_contraction_map(t, sc, sm, A, a->out_map, &sz, &err);
+        if (t.leader()) {
+            a->out_nr = nr;
+            a->out_count = sz;
+            a->status |= err;
+        }
+    } else if (op == RAMA_STEP_MSF) {
+        int32_t mx = team_max<Team, int32_t>(t, sc, sm, a->m, 0, [&](int64_t e) { return max(a->i[e], a->j[e]); });
+        bool ok = team_msf(t, sc, sm, a->m, mx + 1, [&](int64_t e) { return a->i[e]; },
+                           [&](int64_t e) { return a->j[e]; }, [&](int64_t e) { return a->c[e]; }, a->out_flags);
+        if (t.leader() && !ok) a->status |= ERR_ITER_LIMIT;
+    } else if (op == RAMA_STEP_CC) {
+        const int32_t *off = a->offsets;
+        const int32_t nn = a->num_nodes;
+        bool ok = team_cc(
+            t, sc, nn, a->adj_len,
+            [&](int64_t k) {
+                int32_t lo = 0, hi = nn - 1;  // row of entry k: last v with off[v] <= k
+                while (lo < hi) {
+                    int32_t mid = (lo + hi + 1) >> 1;
+                    if (off[mid] <= k)
+                        lo = mid;
+                    else
+                        hi = mid - 1;
+                }
+                return lo;
+            },
+            [&](int64_t k) { return a->adj[k]; }, a->out_map);
+        if (t.leader() && !ok) a->status |= ERR_ITER_LIMIT;
+    } else if (op == RAMA_STEP_CYCLES) {
+        TriBuf tb;
+        conflicted_cycles(t, sc, sm, A, a->max_cycle_length, a->tri_memory_factor, a->tol, tb);
+        if (sc.arena.ok()) {
+            if (tb.num <= a->out_tri_cap)
+                for (int64_t k = t.rank(); k < tb.num; k += t.size()) {
+                    a->out_t1[k] = tb.t1[k];
+                    a->out_t2[k] = tb.t2[k];
+                    a->out_t3[k] = tb.t3[k];
+                }
+            if (t.leader()) {
+                a->out_count = tb.num;
+                a->out_raw = tb.count;
+                if (tb.num > a->out_tri_cap) a->status |= ERR_INVALID_ARG;
+            }
+        }
+    } else if (op == RAMA_STEP_MP) {
+        TriBuf tb;
+        tb.budget = a->T;
+        tb.count = a->T;
+        tb.num = a->T;
+        tb.t1 = sc.arena.take<int32_t>(a->T + 1);
+        tb.t2 = sc.arena.take<int32_t>(a->T + 1);
+        tb.t3 = sc.arena.take<int32_t>(a->T + 1);
+        if (sc.arena.ok()) {
+            for (int64_t k = t.rank(); k < a->T; k += t.size()) {
+                tb.t1[k] = a->t1[k];
+                tb.t2[k] = a->t2[k];
+                tb.t3[k] = a->t3[k];
+            }
+            t.sync();
+            Mp mp;
+            if (mp_build(t, sc, sm, A, tb, mp)) {
+                double lb0 = mp_lower_bound(t, sc, mp);
+                for (int it = 0; it < a->num_iter; ++it) mp_iteration(t, mp);
+                double lb1 = mp_lower_bound(t, sc, mp);
+                Graph g;
+                g.row = mp.row;
+                g.col = mp.col;
+                g.cost = mp.cost;
+                g.n = mp.E;
+                graph_set_dims(t, sc, sm, g);
+                copy_graph_out(t, g, a);
+                if (t.leader()) {
+                    a->out_lb0 = lb0;
+                    a->out_lb1 = lb1;
+                    a->out_count = mp.T;
+                }
+            }
+        }
+    } else if (op == RAMA_STEP_DUAL) {
+        int64_t nt = 0;
+        int oom = 0;
+        double lb = dual_solver(t, sc, sm, A, a->max_cycle_length, a->num_iter, a->tri_memory_factor, a->num_outer,
+                                a->tol, &nt, &oom);
+        copy_graph_out(t, A, a);
+        if (t.leader()) {
+            a->out_lb0 = lb;
+            a->out_raw = nt;
+            a->out_nr = oom;
+        }
+    } else if (op == RAMA_STEP_CSUM) {
+        double s = team_csum(t, sc, a->m, [&](int64_t k) -> double { return (double)a->c[k]; });
+        if (t.leader()) a->out_lb0 = s;
+    } else if (op == RAMA_STEP_SORT) {
+        uint64_t *k1 = sc.arena.take<uint64_t>(a->m + 1), *k2 = sc.arena.take<uint64_t>(a->m + 1);
+        int32_t *v1 = sc.arena.take<int32_t>(a->m + 1), *v2 = sc.arena.take<int32_t>(a->m + 1);
+        if (sc.arena.ok()) {
+            for (int64_t k = t.rank(); k < a->m; k += t.size()) {
+                k1[k] = a->keys[k];
+                v1[k] = a->i[k];
+            }
+            t.sync();
+            team_sort_pairs(t, sc, sm, k1, v1, k2, v2, a->m, a->key_bits);
+            for (int64_t k = t.rank(); k < a->m; k += t.size()) {
+                a->out_keys[k] = k1[k];
+                a->out_map[k] = v1[k];
+            }
+        }
+    }
+    t.sync();
+    if (t.leader()) {
+        if (!sc.arena.ok()) a->status |= ERR_ARENA;
+    }
+}
+
+__global__ void __launch_bounds__(THREADS, 2) k_step_cta(rama_step_args *a, char *ws, uint64_t bytes)
+{
+    extern __shared__ __align__(16) char sm[];
+    BlockTeam t;
+    run_step(t, sm, make_scratch(ws, bytes), a);
+}
+
+__global__ void __launch_bounds__(THREADS, 2) k_step_grid(rama_step_args *a, char *ws, uint64_t bytes)
+{
+    extern __shared__ __align__(16) char sm[];
+    GridTeam t;
+    run_step(t, sm, make_scratch(ws, bytes), a);
+}
+
+// objective: CSUM over edges whose endpoints carry different labels
+__global__ void __launch_bounds__(THREADS, 2) k_objective(const int32_t *I, const int32_t *J, const float *C, int64_t n,
+                                                          const int32_t *lab, double *out, char *ws, uint64_t bytes)
+{
+    extern __shared__ __align__(16) char sm[];
+    GridTeam t;
+    Scratch sc = make_scratch(ws, bytes);
+    double s = team_csum(t, sc, n, [&](int64_t e) -> double { return lab[I[e]] != lab[J[e]] ? (double)C[e] : 0.0; });
+    if (t.leader()) *out = s;
+}
+
+int status_from_bits(int32_t s)
+{
+    if (s == 0) return RAMA_OK;
+    if (s & ERR_INVALID_ARG) return RAMA_ERR_INVALID_ARG;
+    if (s & ERR_ARENA) return RAMA_ERR_OOM;
+    if (s & ERR_BAD_CONTRACTION) return RAMA_ERR_BAD_CONTRACTION;
+    if (s & ERR_ITER_LIMIT) return RAMA_ERR_ITER_LIMIT;
+    return RAMA_ERR_CUDA;
+}
+
+Options to_opts(const rama_options *o)
+{
+    Options r;
+    r.max_cycle_length_lb = o->max_cycle_length_lb;
+    r.num_dual_itr_lb = o->num_dual_itr_lb;
+    r.max_cycle_length_primal = o->max_cycle_length_primal;
+    r.num_dual_itr_primal = o->num_dual_itr_primal;
+    r.num_outer_itr_dual = o->num_outer_itr_dual;
+    r.mean_multiplier_mm = o->mean_multiplier_mm;
+    r.matching_thresh_crossover_ratio = o->matching_thresh_crossover_ratio;
+    r.tri_memory_factor = o->tri_memory_factor;
+    r.only_compute_lb = o->only_compute_lb;
+    r.max_time_sec = o->max_time_sec;
+    r.dump_timeline = o->dump_timeline;
+    r.verbose = o->verbose;
+    r.sanitize_graph = o->sanitize_graph;
+    return r;
+}
+
+}  // namespace
+
+struct rama_context {
+    int device = 0;
+    int sms = 0;
+    int grid_ctas = 0;  // co-resident CTAs of k_solve_grid
+    int cta_per_sm = 0;
+    char *ws = nullptr;
+    uint64_t ws_bytes = 0;
+    uint64_t ws_fixed = 0;  // user-requested size (0 = automatic)
+    Instance *d_inst = nullptr;
+    int32_t inst_cap = 0;
+    int32_t *d_queue = nullptr;
+    int32_t *d_order = nullptr;
+    rama_step_args *d_step = nullptr;
+    double *d_scalar = nullptr;
+    int32_t *d_timeline = nullptr;
+    int64_t tl_cap = 0;
+    std::vector<int32_t> timeline;
+    int32_t tl_rounds = 0;
+    int64_t tl_labels = 0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    rama_stats stats{};
+};
+
+namespace {
+
+int ensure_ws(rama_context *h, uint64_t need)
+{
+    if (h->ws && h->ws_bytes >= need) return RAMA_OK;
+    if (h->ws) {
+        cudaFree(h->ws);
+        h->ws = nullptr;
+        h->ws_bytes = 0;
+    }
+    size_t fr = 0, tot = 0;
+    CU(cudaMemGetInfo(&fr, &tot));
+    uint64_t limit = (uint64_t)((double)fr * 0.92);
+    uint64_t bytes = std::min<uint64_t>(need, limit);
+    bytes = (bytes + 255) & ~uint64_t(255);
+    if (bytes < (4u << 20)) bytes = 4u << 20;
+    if (cudaMalloc(&h->ws, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        h->ws = nullptr;
+        return fail(RAMA_ERR_OOM, "cannot allocate the solver workspace");
+    }
+    h->ws_bytes = bytes;
+    return RAMA_OK;
+}
+
+int ensure_inst(rama_context *h, int32_t count)
+{
+    if (h->inst_cap >= count) return RAMA_OK;
+    if (h->d_inst) cudaFree(h->d_inst);
+    if (h->d_order) cudaFree(h->d_order);
+    h->d_inst = nullptr;
+    h->d_order = nullptr;
+    CU(cudaMalloc(&h->d_inst, sizeof(Instance) * (size_t)count));
+    CU(cudaMalloc(&h->d_order, sizeof(int32_t) * (size_t)count));
+    h->inst_cap = count;
+    return RAMA_OK;
+}
+
+uint64_t ws_estimate(int64_t n_edges) { return (uint64_t)n_edges * 1024ull + (64ull << 20); }
+
+// Launches the solve of the instances already in h->d_inst.  team 1: CTAs.
+int launch_solve(rama_context *h, const Options &o, int32_t count, int team, cudaStream_t st, uint64_t ws_per_cta)
+{
+    if (team == 2) {
+        GridLaunch L{o, h->d_inst, h->ws, h->ws_bytes};
+        void *args[] = {&L};
+        CU(cudaLaunchCooperativeKernel((void *)k_solve_grid, dim3(h->grid_ctas), dim3(THREADS), args, SMEM, st));
+    } else {
+        const int ctas = std::max(1, std::min<int>(count, (int)(h->ws_bytes / ws_per_cta)));
+        CU(cudaMemsetAsync(h->d_queue, 0, sizeof(int32_t), st));
+        CtaLaunch L{o, h->d_inst, h->d_order, count, h->d_queue, h->ws, ws_per_cta};
+        k_solve_cta<<<ctas, THREADS, SMEM, st>>>(L);
+        CU(cudaGetLastError());
+    }
+    return RAMA_OK;
+}
+
+int solve_one(rama_context *h, const int32_t *d_i, const int32_t *d_j, const float *d_c, int64_t n,
+              const rama_options *opts, int32_t *d_labels, int64_t cap, int64_t *num_labels, double *lb,
+              cudaStream_t st)
+{
+    if (!h || !opts || n < 0 || (n > 0 && (!d_i || !d_j || !d_c))) return fail(RAMA_ERR_INVALID_ARG, "bad arguments");
+    Options o = to_opts(opts);
+    int team = opts->team;
+    if (team != 1 && team != 2) team = (n <= BLOCK_TEAM_MAX_EDGES) ? 1 : 2;
+    int rc = ensure_inst(h, 1);
+    if (rc) return rc;
+    // timeline buffer
+    int32_t *tl = nullptr;
+    int64_t tl_cap = 0;
+    if (opts->dump_timeline) {
+        tl_cap = std::min<int64_t>((int64_t)cap * 64, (int64_t)1 << 28);
+        if (h->tl_cap < tl_cap) {
+            if (h->d_timeline) cudaFree(h->d_timeline);
+            CU(cudaMalloc(&h->d_timeline, sizeof(int32_t) * (size_t)tl_cap));
+            h->tl_cap = tl_cap;
+        }
+        tl = h->d_timeline;
+    }
+    uint64_t need = h->ws_fixed ? h->ws_fixed : ws_estimate(n);
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        rc = ensure_ws(h, need);
+        if (rc) return rc;
+        Instance hi{};
+        hi.i = d_i;
+        hi.j = d_j;
+        hi.c = d_c;
+        hi.n = n;
+        hi.labels = d_labels;
+        hi.labels_cap = cap;
+        hi.timeline = tl;
+        hi.timeline_cap = tl_cap;
+        int32_t zero = 0;
+        CU(cudaMemcpyAsync(h->d_inst, &hi, sizeof(Instance), cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(h->d_order, &zero, sizeof(int32_t), cudaMemcpyHostToDevice, st));
+        CU(cudaEventRecord(h->ev0, st));
+        rc = launch_solve(h, o, 1, team, st, h->ws_bytes);
+        if (rc) return rc;
+        CU(cudaEventRecord(h->ev1, st));
+        Instance ho{};
+        CU(cudaMemcpyAsync(&ho, h->d_inst, sizeof(Instance), cudaMemcpyDeviceToHost, st));
+        CU(cudaStreamSynchronize(st));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+        if ((ho.status & ERR_ARENA) && !h->ws_fixed) {
+            size_t fr = 0, tot = 0;
+            cudaMemGetInfo(&fr, &tot);
+            uint64_t grow = std::max<uint64_t>(need * 2, h->ws_bytes * 2);
+            if (h->ws_bytes >= (uint64_t)((double)(fr + h->ws_bytes) * 0.9)) break;
+            need = grow;
+            continue;
+        }
+        h->stats.rounds = ho.rounds;
+        h->stats.matching_rounds = ho.matching_rounds;
+        h->stats.mst_rounds = ho.mst_rounds;
+        h->stats.timeline_rounds = ho.timeline_rounds;
+        h->stats.dual_oom = ho.dual_oom;
+        h->stats.team = team;
+        h->stats.triangles = ho.triangles_initial;
+        h->stats.edges_after_dual = ho.edges_after_dual;
+        h->stats.workspace_peak = ho.arena_peak;
+        h->stats.device_ms = ms;
+        if (opts->dump_timeline && ho.timeline_rounds > 0) {
+            h->tl_rounds = ho.timeline_rounds;
+            h->tl_labels = ho.num_labels;
+            h->timeline.resize((size_t)ho.timeline_rounds * (size_t)ho.num_labels);
+            CU(cudaMemcpy(h->timeline.data(), h->d_timeline, sizeof(int32_t) * h->timeline.size(),
+                          cudaMemcpyDeviceToHost));
+        } else {
+            h->tl_rounds = 0;
+            h->tl_labels = ho.num_labels;
+            h->timeline.clear();
+        }
+        if (num_labels) *num_labels = ho.num_labels;
+        if (lb) *lb = ho.lb;
+        if (ho.status) {
+            std::string msg = "solver status bits " + std::to_string(ho.status);
+            if (ho.status & ERR_INVALID_ARG) msg = "invalid input (negative id, self loop, or label buffer too small)";
+            if (ho.status & ERR_BAD_CONTRACTION) msg = "Found bad contractions";
+            return fail(status_from_bits(ho.status), msg);
+        }
+        return RAMA_OK;
+    }
+    return fail(RAMA_ERR_OOM, "solver workspace exhausted");
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *rama_last_error(void) { return g_err.c_str(); }
+
+int rama_options_init(rama_options *o, const char *mode)
+{
+    if (!o) return RAMA_ERR_INVALID_ARG;
+    o->max_cycle_length_lb = 5;
+    o->num_dual_itr_lb = 10;
+    o->max_cycle_length_primal = 3;
+    o->num_dual_itr_primal = 5;
+    o->num_outer_itr_dual = 1;
+    o->mean_multiplier_mm = 0.05f;
+    o->matching_thresh_crossover_ratio = 0.05f;
+    o->tri_memory_factor = 2.0f;
+    o->only_compute_lb = 0;
+    o->max_time_sec = -1;
+    o->dump_timeline = 0;
+    o->verbose = 0;
+    o->sanitize_graph = 0;
+    o->team = 0;
+    if (!mode) return RAMA_OK;
+    if (!strcmp(mode, "P")) {
+        o->max_cycle_length_lb = 0;
+        o->num_dual_itr_lb = 0;
+        o->max_cycle_length_primal = 0;
+        o->num_dual_itr_primal = 0;
+    } else if (!strcmp(mode, "PD+")) {
+        o->max_cycle_length_lb = 5;
+        o->num_dual_itr_lb = 10;
+        o->max_cycle_length_primal = 5;
+        o->num_dual_itr_primal = 10;
+    } else if (!strcmp(mode, "D")) {
+        o->max_cycle_length_lb = 5;
+        o->num_dual_itr_lb = 10;
+        o->num_outer_itr_dual = 5;
+        o->only_compute_lb = 1;
+    }
+    return RAMA_OK;
+}
+
+int rama_create(int device, uint64_t workspace_bytes, rama_handle *out)
+{
+    if (!out) return fail(RAMA_ERR_INVALID_ARG, "null handle");
+    *out = nullptr;
+    CU(cudaSetDevice(device));
+    rama_context *h = new rama_context();
+    h->device = device;
+    h->ws_fixed = workspace_bytes;
+    cudaDeviceProp p;
+    CU(cudaGetDeviceProperties(&p, device));
+    h->sms = p.multiProcessorCount;
+    int per_sm = 0;
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve_grid, THREADS, SMEM));
+    if (per_sm < 1) {
+        delete h;
+        return fail(RAMA_ERR_CUDA, "solver kernel does not fit on an SM");
+    }
+    h->grid_ctas = per_sm * h->sms;
+    int per_sm_cta = 0;
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_cta, k_solve_cta, THREADS, SMEM));
+    h->cta_per_sm = std::max(1, per_sm_cta);
+    CU(cudaMalloc(&h->d_queue, sizeof(int32_t) * 4));
+    CU(cudaMalloc(&h->d_step, sizeof(rama_step_args)));
+    CU(cudaMalloc(&h->d_scalar, sizeof(double) * 4));
+    CU(cudaEventCreate(&h->ev0));
+    CU(cudaEventCreate(&h->ev1));
+    *out = h;
+    return RAMA_OK;
+}
+
+void rama_destroy(rama_handle h)
+{
+    if (!h) return;
+    cudaSetDevice(h->device);
+    cudaFree(h->ws);
+    cudaFree(h->d_inst);
+    cudaFree(h->d_order);
+    cudaFree(h->d_queue);
+    cudaFree(h->d_step);
+    cudaFree(h->d_scalar);
+    cudaFree(h->d_timeline);
+    cudaEventDestroy(h->ev0);
+    cudaEventDestroy(h->ev1);
+    delete h;
+}
+
+int rama_solve(rama_handle h, const int32_t *d_i, const int32_t *d_j, const float *d_costs, int64_t num_edges,
+               const rama_options *opts, int32_t *d_labels, int64_t labels_cap, int64_t *num_labels, double *lb,
+               void *stream)
+{
+    if (!h) return fail(RAMA_ERR_INVALID_ARG, "null handle");
+    CU(cudaSetDevice(h->device));
+    return solve_one(h, d_i, d_j, d_costs, num_edges, opts, d_labels, labels_cap, num_labels, lb,
+                     (cudaStream_t)stream);
+}
+
+int rama_solve_host(rama_handle h, const int32_t *i, const int32_t *j, const float *costs, int64_t n,
+                    const rama_options *opts, int32_t *labels, int64_t labels_cap, int64_t *num_labels, double *lb,
+                    double *solve_ms)
+{
+    if (!h || !opts || n < 0 || (n > 0 && (!i || !j || !costs))) return fail(RAMA_ERR_INVALID_ARG, "bad arguments");
+    CU(cudaSetDevice(h->device));
+    int32_t mx = -1;
+    for (int64_t e = 0; e < n; ++e) mx = std::max(mx, std::max(i[e], j[e]));
+    const int64_t cap = (int64_t)mx + 1;
+    int32_t *di = nullptr, *dj = nullptr, *dl = nullptr;
+    float *dc = nullptr;
+    const size_t nb = sizeof(int32_t) * (size_t)std::max<int64_t>(n, 1);
+    CU(cudaMalloc(&di, nb));
+    CU(cudaMalloc(&dj, nb));
+    CU(cudaMalloc(&dc, nb));
+    CU(cudaMalloc(&dl, sizeof(int32_t) * (size_t)std::max<int64_t>(cap, 1)));
+    cudaStream_t st = nullptr;
+    CU(cudaMemcpyAsync(di, i, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(dj, j, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(dc, costs, sizeof(float) * n, cudaMemcpyHostToDevice, st));
+    int64_t nl = 0;
+    int rc = solve_one(h, di, dj, dc, n, opts, dl, cap, &nl, lb, st);
+    if (rc == RAMA_OK) {
+        if (nl > labels_cap)
+            rc = fail(RAMA_ERR_INVALID_ARG, "label buffer too small");
+        else if (nl > 0 && cudaMemcpy(labels, dl, sizeof(int32_t) * nl, cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = fail(RAMA_ERR_CUDA, "copying labels failed");
+        if (num_labels) *num_labels = nl;
+        if (solve_ms) *solve_ms = h->stats.device_ms;
+    }
+    cudaFree(di);
+    cudaFree(dj);
+    cudaFree(dc);
+    cudaFree(dl);
+    return rc;
+}
+
+int rama_get_timeline(rama_handle h, int32_t *out, int64_t cap, int32_t *rounds, int64_t *num_labels)
+{
+    if (!h) return fail(RAMA_ERR_INVALID_ARG, "null handle");
+    if (rounds) *rounds = h->tl_rounds;
+    if (num_labels) *num_labels = h->tl_labels;
+    if (out) {
+        if ((int64_t)h->timeline.size() > cap) return fail(RAMA_ERR_INVALID_ARG, "timeline buffer too small");
+        std::memcpy(out, h->timeline.data(), sizeof(int32_t) * h->timeline.size());
+    }
+    return RAMA_OK;
+}
+
+int rama_solve_batch(rama_handle h, const int32_t *d_i, const int32_t *d_j, const float *d_costs,
+                     const int64_t *edge_offsets, int32_t count, const rama_options *opts, int32_t *d_labels,
+                     const int64_t *label_offsets, int64_t *num_labels, double *lbs, int32_t *status, void *stream)
+{
+    if (!h || !opts || count < 0 || !edge_offsets || !label_offsets) return fail(RAMA_ERR_INVALID_ARG, "bad arguments");
+    if (count == 0) return RAMA_OK;
+    CU(cudaSetDevice(h->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc = ensure_inst(h, count);
+    if (rc) return rc;
+    std::vector<Instance> hi(count);
+    std::vector<int32_t> order(count);
+    int64_t emax = 0;
+    for (int32_t k = 0; k < count; ++k) {
+        const int64_t a = edge_offsets[k], b = edge_offsets[k + 1];
+        hi[k] = Instance{};
+        hi[k].i = d_i + a;
+        hi[k].j = d_j + a;
+        hi[k].c = d_costs + a;
+        hi[k].n = b - a;
+        hi[k].labels = d_labels + label_offsets[k];
+        hi[k].labels_cap = label_offsets[k + 1] - label_offsets[k];
+        emax = std::max(emax, b - a);
+        order[k] = k;
+    }
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int32_t x, int32_t y) { return hi[x].n > hi[y].n; });
+    Options o = to_opts(opts);
+    uint64_t per_cta = ws_estimate(emax);
+    per_cta = (per_cta + 4095) & ~uint64_t(4095);
+    const int ctas = std::min<int>(count, h->sms * h->cta_per_sm);
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        rc = ensure_ws(h, per_cta * (uint64_t)ctas);
+        if (rc) return rc;
+        if (h->ws_bytes < per_cta) return fail(RAMA_ERR_OOM, "workspace too small for one instance");
+        CU(cudaMemcpyAsync(h->d_inst, hi.data(), sizeof(Instance) * count, cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(h->d_order, order.data(), sizeof(int32_t) * count, cudaMemcpyHostToDevice, st));
+        CU(cudaEventRecord(h->ev0, st));
+        rc = launch_solve(h, o, count, 1, st, per_cta);
+        if (rc) return rc;
+        CU(cudaEventRecord(h->ev1, st));
+        std::vector<Instance> ho(count);
+        CU(cudaMemcpyAsync(ho.data(), h->d_inst, sizeof(Instance) * count, cudaMemcpyDeviceToHost, st));
+        CU(cudaStreamSynchronize(st));
+        float ms = 0;
+        cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+        bool arena = false;
+        for (auto &x : ho) arena |= (x.status & ERR_ARENA) != 0;
+        if (arena && attempt < 3) {
+            per_cta *= 2;
+            continue;
+        }
+        int worst = RAMA_OK;
+        int64_t peak = 0;
+        for (int32_t k = 0; k < count; ++k) {
+            if (num_labels) num_labels[k] = ho[k].num_labels;
+            if (lbs) lbs[k] = ho[k].lb;
+            if (status) status[k] = status_from_bits(ho[k].status);
+            if (ho[k].status && worst == RAMA_OK) worst = status_from_bits(ho[k].status);
+            peak = std::max<int64_t>(peak, ho[k].arena_peak);
+        }
+        h->stats = rama_stats{};
+        h->stats.team = 1;
+        h->stats.workspace_peak = peak;
+        h->stats.device_ms = ms;
+        if (worst) return fail(worst, "at least one instance failed (see status)");
+        return RAMA_OK;
+    }
+    return fail(RAMA_ERR_OOM, "solver workspace exhausted");
+}
+
+int rama_get_stats(rama_handle h, rama_stats *out)
+{
+    if (!h || !out) return fail(RAMA_ERR_INVALID_ARG, "bad arguments");
+    *out = h->stats;
+    return RAMA_OK;
+}
+
+int rama_objective(rama_handle h, const int32_t *d_i, const int32_t *d_j, const float *d_costs, int64_t n,
+                   const int32_t *d_labels, double *obj, void *stream)
+{
+    if (!h || !obj) return fail(RAMA_ERR_INVALID_ARG, "bad arguments");
+    CU(cudaSetDevice(h->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc = ensure_ws(h, std::max<uint64_t>(h->ws_bytes, (uint64_t)n / 4096 * 16 + (8u << 20)));
+    if (rc) return rc;
+    void *args[] = {(void *)&d_i, (void *)&d_j, (void *)&d_costs, (void *)&n, (void *)&d_labels,
+                    (void *)&h->d_scalar, (void *)&h->ws, (void *)&h->ws_bytes};
+    CU(cudaLaunchCooperativeKernel((void *)k_objective, dim3(h->grid_ctas), dim3(THREADS), args, SMEM, st));
+    CU(cudaMemcpyAsync(obj, h->d_scalar, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    return RAMA_OK;
+}
+
+int rama_step(rama_handle h, rama_step_args *a, void *stream)
+{
+    if (!h || !a) return fail(RAMA_ERR_INVALID_ARG, "bad arguments");
+    CU(cudaSetDevice(h->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    int64_t scale = std::max<int64_t>({a->n, a->m, a->T * 3, a->adj_len, (int64_t)a->num_nodes, a->map_size});
+    int rc = ensure_ws(h, h->ws_fixed ? h->ws_fixed : ws_estimate(scale) + (uint64_t)a->num_nodes * 64);
+    if (rc) return rc;
+    a->status = 0;
+    CU(cudaMemcpyAsync(h->d_step, a, sizeof(rama_step_args), cudaMemcpyHostToDevice, st));
+    if (a->team == 2) {
+        void *args[] = {(void *)&h->d_step, (void *)&h->ws, (void *)&h->ws_bytes};
+        CU(cudaLaunchCooperativeKernel((void *)k_step_grid, dim3(h->grid_ctas), dim3(THREADS), args, SMEM, st));
+    } else {
+        k_step_cta<<<1, THREADS, SMEM, st>>>(h->d_step, h->ws, h->ws_bytes);
+        CU(cudaGetLastError());
+    }
+    CU(cudaMemcpyAsync(a, h->d_step, sizeof(rama_step_args), cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    if (a->status) return fail(status_from_bits(a->status), "step status bits " + std::to_string(a->status));
+    return RAMA_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,263 @@
+// cycles.cuh -- conflicted 3/4/5-cycle search on the CSR of attractive edges
+// (src/conflicted_cycles_cuda.cu:13-343).  Each conflicted cycle is emitted
+// as triangles; the budget keeps the first `budget` emissions in canonical
+// order (rep edge, neighbour/expansion index, common neighbour ascending),
+// computed by count -> scan -> write over chunks of expansions.
+#pragma once
+#include "graph.cuh"
+
+namespace rama {
+
+struct TriBuf {
+    int32_t *t1, *t2, *t3;  // capacity budget + 1
+    int64_t budget;
+    int64_t count;  // the reference's triangle counter (budget+1 once overflowed)
+    int64_t num;    // valid entries: min(count, budget)
+};
+
+__device__ __forceinline__ int count_common(const int32_t *adj, int32_t a0, int32_t a1, int32_t b0, int32_t b1)
+{
+    int c = 0;
+    while (a0 < a1 && b0 < b1) {
+        int32_t x = adj[a0], y = adj[b0];
+        c += (x == y);
+        a0 += (x <= y);
+        b0 += (y <= x);
+    }
+    return c;
+}
+
+template <class F>
+__device__ __forceinline__ void for_common(const int32_t *adj, int32_t a0, int32_t a1, int32_t b0, int32_t b1, F f)
+{
+    while (a0 < a1 && b0 < b1) {
+        int32_t x = adj[a0], y = adj[b0];
+        if (x == y) f(x);
+        a0 += (x <= y);
+        b0 += (y <= x);
+    }
+}
+
+__device__ __forceinline__ void write_tri(TriBuf &tb, int64_t pos, int32_t a, int32_t b, int32_t c)
+{
+    if (pos >= tb.budget) return;
+    int32_t lo = min(a, min(b, c)), hi = max(a, max(b, c));
+    int32_t md = max(min(a, b), min(max(a, b), c));
+    tb.t1[pos] = lo;
+    tb.t2[pos] = md;
+    tb.t3[pos] = hi;
+}
+
+// remove degenerate triangles, sort lexicographically, unique (the first n
+// entries of the buffer); returns the new count
+template <class Team>
+__device__ int64_t tri_normalize(const Team &t, Scratch &sc, char *sm, int32_t *t1, int32_t *t2, int32_t *t3, int64_t n,
+                                 int32_t nmax)
+{
+    if (n == 0) return 0;
+    const int nb = bits_for((uint64_t)(nmax > 0 ? nmax : 1));
+    uint64_t m = sc.arena.mark();
+    uint64_t *k1 = sc.arena.take<uint64_t>(n + 1), *k2 = sc.arena.take<uint64_t>(n + 1);
+    uint64_t *u1 = sc.arena.take<uint64_t>(n + 1), *u2 = sc.arena.take<uint64_t>(n + 1);
+    if (!sc.arena.ok()) return 0;
+    // stable sort by t3 carrying (t1,t2); then by (t1,t2) carrying t3
+    const int64_t w = team_compact(
+        t, sc, sm, n, [&](int64_t k) { return !(t1[k] == t2[k] || t1[k] == t3[k] || t2[k] == t3[k]); },
+        [&](int64_t k, int64_t p) {
+            int32_t a = t1[k], b = t2[k], c = t3[k];
+            int32_t lo = min(a, min(b, c)), hi = max(a, max(b, c));
+            int32_t md = max(min(a, b), min(max(a, b), c));
+            k1[p] = (uint64_t)(uint32_t)hi;
+            u1[p] = pack_key(lo, md, nb);
+        });
+    team_sort_pairs(t, sc, sm, k1, u1, k2, u2, w, nb);
+    for (int64_t k = t.rank(); k < w; k += t.size()) {
+        uint64_t tmp = u1[k];
+        u1[k] = k1[k];  // t3 becomes the value
+        k1[k] = tmp;
+    }
+    t.sync();
+    team_sort_pairs(t, sc, sm, k1, u1, k2, u2, w, 2 * nb);
+    const uint64_t mask = (nb == 0) ? 0 : ((uint64_t(1) << nb) - 1);
+    const int64_t u = team_compact(
+        t, sc, sm, w, [&](int64_t k) { return k == 0 || k1[k] != k1[k - 1] || u1[k] != u1[k - 1]; },
+        [&](int64_t k, int64_t p) {
+            t1[p] = (int32_t)(k1[k] >> nb);
+            t2[p] = (int32_t)(k1[k] & mask);
+            t3[p] = (int32_t)u1[k];
+        });
+    sc.arena.release(m);
+    return u;
+}
+
+// Expansion stage over X expansions (X given as an exclusive scan xo[R+1]
+// over rep edges).  For each expansion: count(x) emissions, then write them
+// at `count + prefix`.  Processed in chunks so that a filled budget stops the
+// work early.
+template <class Team, class Count, class Emit>
+__device__ void expansion_stage(const Team &t, Scratch &sc, char *sm, TriBuf &tb, const int64_t *xo, int64_t R,
+                                int64_t X, Count cnt, Emit emit)
+{
+    const int64_t CH = int64_t(1) << 24;
+    uint64_t m = sc.arena.mark();
+    int32_t *ccount = sc.arena.take<int32_t>(CH < X ? CH : X + 1);
+    int64_t *cbase = sc.arena.take<int64_t>((CH < X ? CH : X) + 1);
+    if (!sc.arena.ok()) return;
+    for (int64_t x0 = 0; x0 < X && tb.count <= tb.budget; x0 += CH) {
+        const int64_t xn = (X - x0) < CH ? (X - x0) : CH;
+        // count
+        for (int64_t q = t.rank(); q < xn; q += t.size()) {
+            int64_t x = x0 + q;
+            int64_t lo = 0, hi = R;  // largest r with xo[r] <= x
+            while (lo < hi) {
+                int64_t mid = (lo + hi + 1) >> 1;
+                if (xo[mid] <= x)
+                    lo = mid;
+                else
+                    hi = mid - 1;
+            }
+            ccount[q] = cnt(lo, x - xo[lo]);
+        }
+        t.sync();
+        const int64_t tot = team_scan<Team, int64_t>(
+            t, sc, sm, xn, [&](int64_t q) -> int64_t { return ccount[q]; },
+            [&](int64_t q, int64_t pre, int64_t) { cbase[q] = pre; });
+        const int64_t start = tb.count;
+        for (int64_t q = t.rank(); q < xn; q += t.size()) {
+            if (ccount[q] == 0 || start + cbase[q] >= tb.budget) continue;
+            int64_t x = x0 + q;
+            int64_t lo = 0, hi = R;
+            while (lo < hi) {
+                int64_t mid = (lo + hi + 1) >> 1;
+                if (xo[mid] <= x)
+                    lo = mid;
+                else
+                    hi = mid - 1;
+            }
+            emit(lo, x - xo[lo], start + cbase[q]);
+        }
+        t.sync();
+        tb.count = start + tot;
+        if (tb.count > tb.budget) tb.count = tb.budget + 1;
+    }
+    sc.arena.release(m);
+}
+
+// conflicted_cycles_cuda (:222-343).  Triangles land in tb (allocated here
+// in the temporaries); tb.count is the reference's counter.
+template <class Team>
+__device__ void conflicted_cycles(const Team &t, Scratch &sc, char *sm, const Graph &A, int max_len, float tri_factor,
+                                  float tol, TriBuf &tb)
+{
+    tb.count = 0;
+    tb.num = 0;
+    tb.budget = 0;
+    tb.t1 = tb.t2 = tb.t3 = nullptr;
+    if (max_len < 3 || A.n == 0) return;
+    const float mn = team_min<Team, float>(t, sc, sm, A.n, 3.4e38f, [&](int64_t e) { return A.cost[e]; });
+    const float thresh = mn * tol;          // determine_threshold (:170-174)
+    const float pos_tol = -1.0f * thresh;   // create_matrices (:176-220)
+    const int32_t N = A.max_dim();
+    int64_t *ridx = sc.arena.take<int64_t>(A.n + 1);
+    if (!sc.arena.ok()) return;
+    const int64_t R = team_compact(
+        t, sc, sm, A.n, [&](int64_t e) { return A.cost[e] < thresh; }, [&](int64_t e, int64_t p) { ridx[p] = e; });
+    const int64_t P = team_sum<Team, int64_t>(t, sc, sm, A.n, [&](int64_t e) -> int64_t { return A.cost[e] > pos_tol; });
+    if (P == 0 || R == 0) return;
+    Csr C = build_symmetric_csr(t, sc, sm, A, N, [&](int64_t e) { return A.cost[e] > pos_tol; }, false);
+    const int64_t budget = (int64_t)(int32_t)(tri_factor * (float)R);  // (:247)
+    tb.budget = budget < 0 ? 0 : budget;
+    tb.t1 = sc.arena.take<int32_t>(tb.budget + 1);
+    tb.t2 = sc.arena.take<int32_t>(tb.budget + 1);
+    tb.t3 = sc.arena.take<int32_t>(tb.budget + 1);
+    int64_t *xo = sc.arena.take<int64_t>(R + 2);
+    if (!sc.arena.ok()) return;
+    const int32_t *off = C.off;
+    const int32_t *adj = C.adj;
+    auto rv1 = [&](int64_t r) { return A.row[ridx[r]]; };
+    auto rv2 = [&](int64_t r) { return A.col[ridx[r]]; };
+    // ---- 3-cycles: find_triangles_parallel (:31-61)
+    {
+        for (int64_t r = t.rank(); r <= R; r += t.size()) xo[r] = r;
+        t.sync();
+        TriBuf &T = tb;
+        expansion_stage(
+            t, sc, sm, T, xo, R, R,
+            [&](int64_t r, int64_t) {
+                int32_t v1 = rv1(r), v2 = rv2(r);
+                return count_common(adj, off[v1], off[v1 + 1], off[v2], off[v2 + 1]);
+            },
+            [&](int64_t r, int64_t, int64_t pos) {
+                int32_t v1 = rv1(r), v2 = rv2(r);
+                for_common(adj, off[v1], off[v1 + 1], off[v2], off[v2 + 1], [&](int32_t mid) {
+                    write_tri(T, pos, v1, v2, mid);
+                    ++pos;
+                });
+            });
+    }
+    // ---- 4-cycles: find_quadrangles_parallel (:63-101)
+    if (max_len >= 4 && tb.count < tb.budget) {
+        tb.count = tri_normalize(t, sc, sm, tb.t1, tb.t2, tb.t3, tb.count, N);
+        const int64_t X = team_scan<Team, int64_t>(
+            t, sc, sm, R, [&](int64_t r) -> int64_t { int32_t v1 = rv1(r); return off[v1 + 1] - off[v1]; },
+            [&](int64_t r, int64_t pre, int64_t) { xo[r] = pre; });
+        if (t.rank() == 0) xo[R] = X;
+        t.sync();
+        TriBuf &T = tb;
+        expansion_stage(
+            t, sc, sm, T, xo, R, X,
+            [&](int64_t r, int64_t loc) {
+                int32_t v1 = rv1(r), v2 = rv2(r);
+                int32_t n1 = adj[off[v1] + loc];
+                return 2 * count_common(adj, off[n1], off[n1 + 1], off[v2], off[v2 + 1]);
+            },
+            [&](int64_t r, int64_t loc, int64_t pos) {
+                int32_t v1 = rv1(r), v2 = rv2(r);
+                int32_t n1 = adj[off[v1] + loc];
+                for_common(adj, off[n1], off[n1 + 1], off[v2], off[v2 + 1], [&](int32_t mid) {
+                    write_tri(T, pos, v1, v2, n1);
+                    write_tri(T, pos + 1, v2, n1, mid);
+                    pos += 2;
+                });
+            });
+    }
+    // ---- 5-cycles: find_pentagons_parallel (:103-148)
+    if (max_len >= 5 && tb.count < tb.budget) {
+        tb.count = tri_normalize(t, sc, sm, tb.t1, tb.t2, tb.t3, tb.count, N);
+        const int64_t X = team_scan<Team, int64_t>(
+            t, sc, sm, R,
+            [&](int64_t r) -> int64_t {
+                int32_t v1 = rv1(r), v2 = rv2(r);
+                return (int64_t)(off[v1 + 1] - off[v1]) * (int64_t)(off[v2 + 1] - off[v2]);
+            },
+            [&](int64_t r, int64_t pre, int64_t) { xo[r] = pre; });
+        if (t.rank() == 0) xo[R] = X;
+        t.sync();
+        TriBuf &T = tb;
+        expansion_stage(
+            t, sc, sm, T, xo, R, X,
+            [&](int64_t r, int64_t loc) {
+                int32_t v1 = rv1(r), v2 = rv2(r);
+                int64_t d1 = off[v1 + 1] - off[v1];
+                int32_t n1 = adj[off[v1] + (int32_t)(loc % d1)];
+                int32_t n2 = adj[off[v2] + (int32_t)(loc / d1)];
+                if (n1 == n2) return 0;
+                return 3 * count_common(adj, off[n1], off[n1 + 1], off[n2], off[n2 + 1]);
+            },
+            [&](int64_t r, int64_t loc, int64_t pos) {
+                int32_t v1 = rv1(r), v2 = rv2(r);
+                int64_t d1 = off[v1 + 1] - off[v1];
+                int32_t n1 = adj[off[v1] + (int32_t)(loc % d1)];
+                int32_t n2 = adj[off[v2] + (int32_t)(loc / d1)];
+                for_common(adj, off[n1], off[n1 + 1], off[n2], off[n2 + 1], [&](int32_t mid) {
+                    write_tri(T, pos, v1, v2, n1);
+                    write_tri(T, pos + 1, v2, n1, mid);
+                    write_tri(T, pos + 2, v2, mid, n2);
+                    pos += 3;
+                });
+            });
+    }
+    tb.num = tb.count < tb.budget ? tb.count : tb.budget;
+}
+
+}  // namespace rama

@@ -1,0 +1,375 @@
+// graph.cuh -- the device graph store (directed COO, row<col, sorted by
+// (row,col)) and its coarsening.  Restates dCOO (include/dCOO.h:13-121,
+// src/dCOO.cu:14-172) with one radix sort of packed (row,col) keys per
+// coarsening and a deterministic segmented sum of parallel edges.
+#pragma once
+#include "prims.cuh"
+
+namespace rama {
+
+struct Graph {
+    int32_t *row, *col;
+    float *cost;
+    int64_t n;
+    int32_t rows, cols;  // dCOO::rows_ / cols_
+    __device__ __forceinline__ int32_t max_dim() const { return rows > cols ? rows : cols; }
+};
+
+// Scratch arrays of a new graph, allocated in the temporaries.
+template <class Team>
+__device__ Graph graph_alloc(const Team &t, Scratch &sc, int64_t n)
+{
+    Graph g;
+    g.row = sc.arena.take<int32_t>(n + 1);
+    g.col = sc.arena.take<int32_t>(n + 1);
+    g.cost = sc.arena.take<float>(n + 1);
+    g.n = n;
+    g.rows = g.cols = 0;
+    return g;
+}
+
+// Move a graph built in the temporaries into the top slot of the arena
+// (the slot ends at the arena's end; the old graph there is dead).  Fails
+// (team-uniformly) if the slot would overlap live temporaries.
+template <class Team>
+__device__ Graph graph_commit(const Team &t, Scratch &sc, const Graph &src)
+{
+    Arena &a = sc.arena;
+    uint64_t bytes = (uint64_t)(src.n + 1) * 12 + 3 * 256;
+    uint64_t top = (a.cap - bytes) & ~uint64_t(255);
+    Graph g = src;
+    if (a.failed || bytes > a.cap || top < a.lo) {
+        a.failed = 1;
+        return src;
+    }
+    g.row = reinterpret_cast<int32_t *>(a.base + top);
+    g.col = reinterpret_cast<int32_t *>(a.base + top + ((uint64_t)(src.n + 1) * 4 + 255) / 256 * 256);
+    g.cost = reinterpret_cast<float *>(a.base + top + 2 * (((uint64_t)(src.n + 1) * 4 + 255) / 256 * 256));
+    // source lies in the temporaries, strictly below `top`: no overlap
+    for (int64_t e = t.rank(); e < src.n; e += t.size()) {
+        g.row[e] = src.row[e];
+        g.col[e] = src.col[e];
+        g.cost[e] = src.cost[e];
+    }
+    a.top = top;
+    t.sync();
+    return g;
+}
+
+// dims as in dCOO::init (src/dCOO.cu:47-51): rows = last row + 1,
+// cols = max col + 1 (0 for an empty graph)
+template <class Team>
+__device__ void graph_set_dims(const Team &t, Scratch &sc, char *sm, Graph &g)
+{
+    if (g.n == 0) {
+        g.rows = g.cols = 0;
+        return;
+    }
+    int32_t mc = team_max<Team, int32_t>(t, sc, sm, g.n, -1, [&](int64_t e) { return g.col[e]; });
+    g.cols = mc + 1;
+    g.rows = uread(&g.row[g.n - 1]) + 1;
+}
+
+__device__ __forceinline__ uint64_t pack_key(int32_t a, int32_t b, int nbits)
+{
+    return ((uint64_t)(uint32_t)a << nbits) | (uint32_t)b;
+}
+
+// dCOO ctor with unsorted input (src/dCOO.cu:38-45): endpoints ordered,
+// sorted by (row,col), stable.  Inputs are (i, j, c) of length n.
+template <class Team>
+__device__ Graph graph_from_edges(const Team &t, Scratch &sc, char *sm, const int32_t *i, const int32_t *j,
+                                  const float *c, int64_t n)
+{
+    Graph out;
+    out.n = n;
+    out.rows = out.cols = 0;
+    int32_t mx = team_max<Team, int32_t>(t, sc, sm, n, 0, [&](int64_t e) { return i[e] > j[e] ? i[e] : j[e]; });
+    const int nb = bits_for((uint64_t)mx);
+    uint64_t m = sc.arena.mark();
+    uint64_t *k1 = sc.arena.take<uint64_t>(n + 1), *k2 = sc.arena.take<uint64_t>(n + 1);
+    float *v1 = sc.arena.take<float>(n + 1), *v2 = sc.arena.take<float>(n + 1);
+    Graph g = graph_alloc(t, sc, n);
+    if (!sc.arena.ok()) return out;
+    for (int64_t e = t.rank(); e < n; e += t.size()) {
+        int32_t a = i[e], b = j[e];
+        k1[e] = pack_key(a < b ? a : b, a < b ? b : a, nb);
+        v1[e] = c[e];
+    }
+    t.sync();
+    team_sort_pairs(t, sc, sm, k1, v1, k2, v2, n, 2 * nb);
+    const uint64_t mask = (nb == 0) ? 0 : ((uint64_t(1) << nb) - 1);
+    for (int64_t e = t.rank(); e < n; e += t.size()) {
+        g.row[e] = (int32_t)(k1[e] >> nb);
+        g.col[e] = (int32_t)(k1[e] & mask);
+        g.cost[e] = v1[e];
+    }
+    t.sync();
+    graph_set_dims(t, sc, sm, g);
+    Graph r = graph_commit(t, sc, g);
+    sc.arena.release(m);
+    return r;
+}
+
+// dCOO::contract_cuda (src/dCOO.cu:57-95) followed by has_bad_contractions
+// (src/rama_cuda.cu:18-30) and remove_diagonal (src/dCOO.cu:106-116).
+// Parallel edges are summed in sorted (stable) order with RSUM.
+// Returns the new graph (committed to the top slot); *bad is set if a
+// self-loop of negative cost appeared.  Dims are taken before the diagonal
+// is removed, as the reference does.
+template <class Team>
+__device__ Graph graph_contract(const Team &t, Scratch &sc, char *sm, const Graph &A, const int32_t *map,
+                                int32_t map_max, int *bad)
+{
+    const int64_t n = A.n;
+    const int nb = bits_for((uint64_t)(map_max > 0 ? map_max : 0));
+    uint64_t m = sc.arena.mark();
+    uint64_t *k1 = sc.arena.take<uint64_t>(n + 1), *k2 = sc.arena.take<uint64_t>(n + 1);
+    float *v1 = sc.arena.take<float>(n + 1), *v2 = sc.arena.take<float>(n + 1);
+    int64_t *runpos = sc.arena.take<int64_t>(n + 2);
+    int32_t *badflag = sc.arena.take<int32_t>(2);
+    Graph out = A;
+    if (!sc.arena.ok()) return out;
+    for (int64_t e = t.rank(); e < n; e += t.size()) {
+        int32_t a = map[A.row[e]], b = map[A.col[e]];
+        k1[e] = pack_key(a < b ? a : b, a < b ? b : a, nb);
+        v1[e] = A.cost[e];
+    }
+    if (t.rank() == 0) badflag[0] = 0;
+    t.sync();
+    team_sort_pairs(t, sc, sm, k1, v1, k2, v2, n, 2 * nb);
+    // run heads -> run index
+    const int64_t nruns = team_compact(
+        t, sc, sm, n, [&](int64_t k) { return k == 0 || k1[k] != k1[k - 1]; },
+        [&](int64_t k, int64_t r) { runpos[r] = k; });
+    if (t.rank() == 0) runpos[nruns] = n;
+    t.sync();
+    Graph g = graph_alloc(t, sc, nruns);
+    int32_t *longq = sc.arena.take<int32_t>(nruns + 1);
+    int32_t *nlong = sc.arena.take<int32_t>(2);
+    if (!sc.arena.ok()) return out;
+    const uint64_t mask = (nb == 0) ? 0 : ((uint64_t(1) << nb) - 1);
+    if (t.rank() == 0) nlong[0] = 0;
+    t.sync();
+    for (int64_t r = t.rank(); r < nruns; r += t.size()) {
+        int64_t s = runpos[r], e = runpos[r + 1];
+        uint64_t key = k1[s];
+        g.row[r] = (int32_t)(key >> nb);
+        g.col[r] = (int32_t)(key & mask);
+        if (e - s <= 32) {
+            g.cost[r] = rsum_serial((int)(e - s), [&](int k) { return v1[s + k]; });
+        } else {
+            int q = atomicAdd(nlong, 1);
+            longq[q] = (int32_t)r;
+        }
+    }
+    t.sync();
+    const int32_t nl = uread(nlong);
+    for (int64_t q = team_warp(t); q < nl; q += team_nwarps(t)) {
+        int64_t r = longq[q];
+        int64_t s = runpos[r], e = runpos[r + 1];
+        float v = rsum_warp(e - s, [&](int64_t k) { return v1[s + k]; });
+        if (lane_id() == 0) g.cost[r] = v;
+    }
+    t.sync();
+    g.n = nruns;
+    graph_set_dims(t, sc, sm, g);
+    // bad contractions + stable removal of the diagonal
+    for (int64_t r = t.rank(); r < nruns; r += t.size())
+        if (g.row[r] == g.col[r] && g.cost[r] < 0.0f) badflag[0] = 1;
+    Graph h = graph_alloc(t, sc, nruns);
+    if (!sc.arena.ok()) return out;
+    const int64_t nk = team_compact(
+        t, sc, sm, nruns, [&](int64_t r) { return g.row[r] != g.col[r]; },
+        [&](int64_t r, int64_t p) {
+            h.row[p] = g.row[r];
+            h.col[p] = g.col[r];
+            h.cost[p] = g.cost[r];
+        });
+    *bad = uread(badflag);
+    h.n = nk;
+    h.rows = g.rows;
+    h.cols = g.cols;
+    Graph res = graph_commit(t, sc, h);
+    sc.arena.release(m);
+    return res;
+}
+
+// Stable contraction WITHOUT diagonal removal (the raw contract_cuda result,
+// for parity tests); result lives in the temporaries.
+template <class Team>
+__device__ Graph graph_contract_raw(const Team &t, Scratch &sc, char *sm, const Graph &A, const int32_t *map,
+                                    int32_t map_max)
+{
+    const int64_t n = A.n;
+    const int nb = bits_for((uint64_t)(map_max > 0 ? map_max : 0));
+    uint64_t *k1 = sc.arena.take<uint64_t>(n + 1), *k2 = sc.arena.take<uint64_t>(n + 1);
+    float *v1 = sc.arena.take<float>(n + 1), *v2 = sc.arena.take<float>(n + 1);
+    int64_t *runpos = sc.arena.take<int64_t>(n + 2);
+    Graph out = A;
+    if (!sc.arena.ok()) return out;
+    for (int64_t e = t.rank(); e < n; e += t.size()) {
+        int32_t a = map[A.row[e]], b = map[A.col[e]];
+        k1[e] = pack_key(a < b ? a : b, a < b ? b : a, nb);
+        v1[e] = A.cost[e];
+    }
+    t.sync();
+    team_sort_pairs(t, sc, sm, k1, v1, k2, v2, n, 2 * nb);
+    const int64_t nruns = team_compact(
+        t, sc, sm, n, [&](int64_t k) { return k == 0 || k1[k] != k1[k - 1]; },
+        [&](int64_t k, int64_t r) { runpos[r] = k; });
+    if (t.rank() == 0) runpos[nruns] = n;
+    t.sync();
+    Graph g = graph_alloc(t, sc, nruns);
+    if (!sc.arena.ok()) return out;
+    const uint64_t mask = (nb == 0) ? 0 : ((uint64_t(1) << nb) - 1);
+    for (int64_t r = t.rank(); r < nruns; r += t.size()) {
+        int64_t s = runpos[r], e = runpos[r + 1];
+        uint64_t key = k1[s];
+        g.row[r] = (int32_t)(key >> nb);
+        g.col[r] = (int32_t)(key & mask);
+        g.cost[r] = (e - s <= 32) ? rsum_serial((int)(e - s), [&](int k) { return v1[s + k]; }) : 0.0f;
+    }
+    t.sync();
+    for (int64_t r = team_warp(t); r < nruns; r += team_nwarps(t)) {
+        int64_t s = runpos[r], e = runpos[r + 1];
+        if (e - s <= 32) continue;
+        float v = rsum_warp(e - s, [&](int64_t k) { return v1[s + k]; });
+        if (lane_id() == 0) g.cost[r] = v;
+    }
+    t.sync();
+    g.n = nruns;
+    graph_set_dims(t, sc, sm, g);
+    return g;
+}
+
+// ---------------------------------------------------------------------------
+// Symmetric CSR of a (row,col)-sorted directed edge list restricted to the
+// edges where keep(e) holds: row v lists its neighbours u<v (increasing u)
+// then w>v (increasing w) -- the (row,col) order of the doubled list
+// (to_undirected + coo_sorting, include/rama_utils.h:107-131, 287-294).
+// Built with one stable radix sort of the kept edges by column.
+// ---------------------------------------------------------------------------
+struct Csr {
+    int32_t nrows;
+    int32_t *off;  // nrows + 1
+    int32_t *adj;  // 2m
+    float *w;      // 2m
+    int32_t *eid;  // 2m: index of the directed edge (in the kept order) -- optional
+    int64_t m2;
+};
+
+template <class Team, class Keep>
+__device__ Csr build_symmetric_csr(const Team &t, Scratch &sc, char *sm, const Graph &A, int32_t nrows, Keep keep,
+                                   bool with_eid, int64_t *kept_idx_out = nullptr)
+{
+    Csr C;
+    C.nrows = nrows;
+    C.m2 = 0;
+    // 1. compact kept edges (their order stays (row,col)-sorted)
+    int64_t *kidx = kept_idx_out ? kept_idx_out : sc.arena.take<int64_t>(A.n + 1);
+    int32_t *deg = sc.arena.take<int32_t>((int64_t)nrows + 1);
+    C.off = sc.arena.take<int32_t>((int64_t)nrows + 2);
+    if (!sc.arena.ok()) return C;
+    for (int64_t v = t.rank(); v <= nrows; v += t.size()) deg[v] = 0;
+    const int64_t m = team_compact(t, sc, sm, A.n, keep, [&](int64_t e, int64_t p) { kidx[p] = e; });
+    C.m2 = 2 * m;
+    C.adj = sc.arena.take<int32_t>(2 * m + 1);
+    C.w = sc.arena.take<float>(2 * m + 1);
+    C.eid = with_eid ? sc.arena.take<int32_t>(2 * m + 1) : nullptr;
+    uint64_t mk = sc.arena.mark();
+    uint64_t *k1 = sc.arena.take<uint64_t>(m + 1), *k2 = sc.arena.take<uint64_t>(m + 1);
+    int32_t *v1 = sc.arena.take<int32_t>(m + 1), *v2 = sc.arena.take<int32_t>(m + 1);
+    int32_t *infill = sc.arena.take<int32_t>((int64_t)nrows + 1);
+    if (!sc.arena.ok()) return C;
+    // 2. degrees (in + out) and in-degrees (number of u<v entries per row)
+    for (int64_t v = t.rank(); v <= nrows; v += t.size()) infill[v] = 0;
+    t.sync();
+    for (int64_t p = t.rank(); p < m; p += t.size()) {
+        int64_t e = kidx[p];
+        atomicAdd(&deg[A.row[e]], 1);
+        atomicAdd(&deg[A.col[e]], 1);
+        atomicAdd(&infill[A.col[e]], 1);
+        k1[p] = (uint64_t)(uint32_t)A.col[e];
+        v1[p] = (int32_t)p;
+    }
+    t.sync();
+    team_scan<Team, int64_t>(
+        t, sc, sm, (int64_t)nrows, [&](int64_t v) -> int64_t { return deg[v]; },
+        [&](int64_t v, int64_t pre, int64_t) { C.off[v] = (int32_t)pre; });
+    if (t.rank() == 0) C.off[nrows] = (int32_t)(2 * m);
+    t.sync();
+    // 3. stable sort of kept edges by column -> reverse entries in increasing row order
+    team_sort_pairs(t, sc, sm, k1, v1, k2, v2, m, bits_for((uint64_t)(nrows > 0 ? nrows : 1)));
+    for (int64_t q = t.rank(); q < m; q += t.size()) {
+        int32_t c = (int32_t)k1[q];
+        // position inside the run: binary search for the run start
+        int64_t lo = 0, hi = q;
+        while (lo < hi) {
+            int64_t mid = (lo + hi) >> 1;
+            if ((int32_t)k1[mid] < c)
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
+        int64_t p = v1[q];
+        int64_t e = kidx[p];
+        int64_t dst = (int64_t)C.off[c] + (q - lo);
+        C.adj[dst] = A.row[e];
+        C.w[dst] = A.cost[e];
+        if (with_eid) C.eid[dst] = (int32_t)p;
+    }
+    // forward entries: the kept edges of row r are contiguous in kidx order
+    for (int64_t p = t.rank(); p < m; p += t.size()) {
+        int64_t e = kidx[p];
+        int32_t r = A.row[e];
+        int64_t lo = 0, hi = p;  // first kept index with row r
+        while (lo < hi) {
+            int64_t mid = (lo + hi) >> 1;
+            if (A.row[kidx[mid]] < r)
+                lo = mid + 1;
+            else
+                hi = mid;
+        }
+        int64_t dst = (int64_t)C.off[r] + infill[r] + (p - lo);
+        C.adj[dst] = A.col[e];
+        C.w[dst] = A.cost[e];
+        if (with_eid) C.eid[dst] = (int32_t)p;
+    }
+    t.sync();
+    sc.arena.release(mk);
+    return C;
+}
+
+// lower bound of the directed graph: sum of min(0, c) (get_lb,
+// include/rama_utils.h:179-190), CSUM
+template <class Team>
+__device__ double graph_lb(const Team &t, Scratch &sc, const Graph &A)
+{
+    return team_csum(t, sc, A.n, [&](int64_t e) -> double {
+        float c = A.cost[e];
+        return c < 0.0f ? (double)c : 0.0;
+    });
+}
+
+// compress_label_sequence (include/rama_utils.h:160-177)
+template <class Team>
+__device__ void compress_labels(const Team &t, Scratch &sc, char *sm, const int32_t *data, int64_t n,
+                                int32_t max_label, int32_t *out)
+{
+    uint64_t m = sc.arena.mark();
+    int32_t *mask = sc.arena.take<int32_t>((int64_t)max_label + 2);
+    if (!sc.arena.ok()) return;
+    for (int64_t l = t.rank(); l <= max_label; l += t.size()) mask[l] = 0;
+    t.sync();
+    for (int64_t k = t.rank(); k < n; k += t.size()) mask[data[k]] = 1;
+    t.sync();
+    team_scan<Team, int64_t>(
+        t, sc, sm, (int64_t)max_label + 1, [&](int64_t l) -> int64_t { return mask[l]; },
+        [&](int64_t l, int64_t pre, int64_t) { mask[l] = (int32_t)pre; });
+    for (int64_t k = t.rank(); k < n; k += t.size()) out[k] = mask[data[k]];
+    t.sync();
+    sc.arena.release(m);
+}
+
+}  // namespace rama

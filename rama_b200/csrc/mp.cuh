@@ -1,0 +1,360 @@
+// mp.cuh -- triangle message passing (src/multicut_message_passing.cu:15-360)
+// and the dual solver loop (src/dual_solver.cu:7-63).
+//
+// Layout (all SoA in the arena): triangles t1<t2<t3 sorted and unique; their
+// edge indices e12/e13/e23 into the merged edge list (the graph's edges plus
+// the triangle chords it lacks, cost 0); per-edge incidence lists (3t+slot,
+// in triangle order) that replace the reference's float atomicAdd by a
+// deterministic RSUM per edge.
+#pragma once
+#include "cycles.cuh"
+
+namespace rama {
+
+struct Mp {
+    int64_t T, E;
+    int32_t *t1, *t2, *t3;
+    int32_t *e12, *e13, *e23;
+    float *c12, *c13, *c23;
+    float *diff;  // 3T
+    int32_t *row, *col;
+    float *cost;
+    int32_t *inc_off;  // E + 1
+    int32_t *inc;      // 3T
+    int32_t rows, cols;
+};
+
+// position of (a,b) in a (row,col)-sorted list with row offsets `off`
+__device__ __forceinline__ int64_t find_edge(const int32_t *off, const int32_t *col, int32_t a, int32_t b)
+{
+    int32_t lo = off[a], hi = off[a + 1];
+    while (lo < hi) {
+        int32_t m = (lo + hi) >> 1;
+        if (col[m] < b)
+            lo = m + 1;
+        else
+            hi = m;
+    }
+    return (lo < off[a + 1] && col[lo] == b) ? lo : -1;
+}
+
+// number of entries of row a with col < b, plus all rows < a
+__device__ __forceinline__ int64_t lower_edge(const int32_t *off, const int32_t *col, int32_t a, int32_t b)
+{
+    int32_t lo = off[a], hi = off[a + 1];
+    while (lo < hi) {
+        int32_t m = (lo + hi) >> 1;
+        if (col[m] < b)
+            lo = m + 1;
+        else
+            hi = m;
+    }
+    return lo;
+}
+
+// multicut_message_passing ctor (:65-176)
+template <class Team>
+__device__ bool mp_build(const Team &t, Scratch &sc, char *sm, const Graph &A, TriBuf &tb, Mp &mp)
+{
+    int32_t nmax = A.max_dim();
+    // normalize_triangles (:79)
+    const int64_t T = tri_normalize(t, sc, sm, tb.t1, tb.t2, tb.t3, tb.num, nmax);
+    if (!sc.arena.ok()) return false;
+    mp.T = T;
+    mp.t1 = tb.t1;
+    mp.t2 = tb.t2;
+    mp.t3 = tb.t3;
+    // row offsets of A over [0, nmax]
+    int32_t *aoff = sc.arena.take<int32_t>((int64_t)nmax + 2);
+    uint64_t *nk1 = sc.arena.take<uint64_t>(3 * T + 1), *nk2 = sc.arena.take<uint64_t>(3 * T + 1);
+    int32_t *nv1 = sc.arena.take<int32_t>(3 * T + 1), *nv2 = sc.arena.take<int32_t>(3 * T + 1);
+    if (!sc.arena.ok()) return false;
+    team_offsets(t, A.n, nmax, [&](int64_t e) { return A.row[e]; }, aoff);
+    const int nb = bits_for((uint64_t)(nmax > 0 ? nmax : 1));
+    // chords not in A
+    const int64_t nn = team_compact(
+        t, sc, sm, 3 * T,
+        [&](int64_t q) {
+            int64_t k = q / 3;
+            int s = (int)(q % 3);
+            int32_t a = s == 2 ? mp.t2[k] : mp.t1[k];
+            int32_t b = s == 0 ? mp.t2[k] : mp.t3[k];
+            return find_edge(aoff, A.col, a, b) < 0;
+        },
+        [&](int64_t q, int64_t p) {
+            int64_t k = q / 3;
+            int s = (int)(q % 3);
+            int32_t a = s == 2 ? mp.t2[k] : mp.t1[k];
+            int32_t b = s == 0 ? mp.t2[k] : mp.t3[k];
+            nk1[p] = pack_key(a, b, nb);
+            nv1[p] = 0;
+        });
+    team_sort_pairs(t, sc, sm, nk1, nv1, nk2, nv2, nn, 2 * nb);
+    uint64_t *nu = nk2;  // unique chords
+    const int64_t nu_n = team_compact(
+        t, sc, sm, nn, [&](int64_t k) { return k == 0 || nk1[k] != nk1[k - 1]; },
+        [&](int64_t k, int64_t p) { nu[p] = nk1[k]; });
+    // merged edge list (set_union_by_key, :130-158)
+    const int64_t E = A.n + nu_n;
+    mp.E = E;
+    mp.row = sc.arena.take<int32_t>(E + 1);
+    mp.col = sc.arena.take<int32_t>(E + 1);
+    mp.cost = sc.arena.take<float>(E + 1);
+    if (!sc.arena.ok()) return false;
+    const uint64_t mask = (nb == 0) ? 0 : ((uint64_t(1) << nb) - 1);
+    for (int64_t e = t.rank(); e < A.n; e += t.size()) {
+        uint64_t key = pack_key(A.row[e], A.col[e], nb);
+        int64_t lo = 0, hi = nu_n;  // chords < key
+        while (lo < hi) {
+            int64_t m = (lo + hi) >> 1;
+            if (nu[m] < key)
+                lo = m + 1;
+            else
+                hi = m;
+        }
+        int64_t p = e + lo;
+        mp.row[p] = A.row[e];
+        mp.col[p] = A.col[e];
+        mp.cost[p] = A.cost[e];
+    }
+    for (int64_t k = t.rank(); k < nu_n; k += t.size()) {
+        int32_t a = (int32_t)(nu[k] >> nb), b = (int32_t)(nu[k] & mask);
+        int64_t p = k + lower_edge(aoff, A.col, a, b);
+        mp.row[p] = a;
+        mp.col[p] = b;
+        mp.cost[p] = 0.0f;
+    }
+    t.sync();
+    // merged row offsets, correspondences (compute_triangle_edge_correspondence, :15-62)
+    int32_t *moff = aoff;  // reuse
+    team_offsets(t, E, nmax, [&](int64_t e) { return mp.row[e]; }, moff);
+    mp.e12 = sc.arena.take<int32_t>(T + 1);
+    mp.e13 = sc.arena.take<int32_t>(T + 1);
+    mp.e23 = sc.arena.take<int32_t>(T + 1);
+    mp.c12 = sc.arena.take<float>(T + 1);
+    mp.c13 = sc.arena.take<float>(T + 1);
+    mp.c23 = sc.arena.take<float>(T + 1);
+    mp.diff = sc.arena.take<float>(3 * T + 1);
+    mp.inc = sc.arena.take<int32_t>(3 * T + 1);
+    mp.inc_off = sc.arena.take<int32_t>(E + 2);
+    uint64_t ik = sc.arena.mark();
+    uint64_t *q1 = sc.arena.take<uint64_t>(3 * T + 1), *q2 = sc.arena.take<uint64_t>(3 * T + 1);
+    int32_t *w2 = sc.arena.take<int32_t>(3 * T + 1);
+    if (!sc.arena.ok()) return false;
+    for (int64_t k = t.rank(); k < T; k += t.size()) {
+        int32_t a = mp.t1[k], b = mp.t2[k], c = mp.t3[k];
+        int32_t x = (int32_t)find_edge(moff, mp.col, a, b);
+        int32_t y = (int32_t)find_edge(moff, mp.col, a, c);
+        int32_t z = (int32_t)find_edge(moff, mp.col, b, c);
+        mp.e12[k] = x;
+        mp.e13[k] = y;
+        mp.e23[k] = z;
+        mp.c12[k] = mp.c13[k] = mp.c23[k] = 0.0f;
+        q1[3 * k] = (uint64_t)x;
+        q1[3 * k + 1] = (uint64_t)y;
+        q1[3 * k + 2] = (uint64_t)z;
+        mp.inc[3 * k] = (int32_t)(3 * k);
+        mp.inc[3 * k + 1] = (int32_t)(3 * k + 1);
+        mp.inc[3 * k + 2] = (int32_t)(3 * k + 2);
+    }
+    t.sync();
+    // incidence lists: stable sort of (edge, 3t+slot) by edge
+    int32_t *incp = mp.inc;
+    uint64_t *qk = q1;
+    team_sort_pairs(t, sc, sm, qk, incp, q2, w2, 3 * T, bits_for((uint64_t)(E > 0 ? E : 1)));
+    if (incp != mp.inc) {
+        for (int64_t k = t.rank(); k < 3 * T; k += t.size()) mp.inc[k] = incp[k];
+    }
+    team_offsets(t, 3 * T, (int32_t)E, [&](int64_t k) { return (int32_t)qk[k]; }, mp.inc_off);
+    sc.arena.release(ik);
+    mp.rows = A.rows;
+    mp.cols = A.cols;
+    return true;
+}
+
+// triangle_lb_func (:186-199)
+__device__ __forceinline__ float tri_lb(float c12, float c13, float c23)
+{
+    float lb = 0.0f;
+    lb = fminf(lb, __fadd_rn(c12, c13));
+    lb = fminf(lb, __fadd_rn(c12, c23));
+    lb = fminf(lb, __fadd_rn(c13, c23));
+    lb = fminf(lb, __fadd_rn(__fadd_rn(c12, c13), c23));
+    return lb;
+}
+
+// lower_bound (:201-216), CSUM for both parts
+template <class Team>
+__device__ double mp_lower_bound(const Team &t, Scratch &sc, const Mp &mp)
+{
+    double le = team_csum(t, sc, mp.E, [&](int64_t e) -> double {
+        float c = mp.cost[e];
+        return c < 0.0f ? (double)c : 0.0;
+    });
+    double lt = team_csum(t, sc, mp.T, [&](int64_t k) -> double { return (double)tri_lb(mp.c12[k], mp.c13[k], mp.c23[k]); });
+    return le + lt;
+}
+
+// decrease_triangle_costs_func::min_marginal (:275-280)
+__device__ __forceinline__ float min_marginal(float x, float y, float z)
+{
+    float mm1 = fminf(__fadd_rn(__fadd_rn(x, y), z), fminf(__fadd_rn(x, y), __fadd_rn(x, z)));
+    float yz = __fadd_rn(y, z);
+    float mm0 = (0.0 < (double)yz) ? 0.0f : yz;
+    return __fsub_rn(mm1, mm0);
+}
+
+__device__ __forceinline__ float sub_scaled(float a, double s, float mm)
+{
+    return (float)__dsub_rn((double)a, __dmul_rn(s, (double)mm));
+}
+__device__ __forceinline__ float add_scaled(float a, double s, float mm)
+{
+    return (float)__dadd_rn((double)a, __dmul_rn(s, (double)mm));
+}
+
+// one iteration (:350-354): send_messages_to_triplets (:241-269) fused with
+// the six min-marginal moves of send_messages_to_edges (:271-348); then each
+// covered edge takes the RSUM of its incoming messages.
+template <class Team>
+__device__ void mp_iteration(const Team &t, const Mp &mp)
+{
+    const double third = 1.0 / 3.0, half = 1.0 / 2.0;
+    for (int64_t k = t.rank(); k < mp.T; k += t.size()) {
+        const int32_t x = mp.e12[k], y = mp.e13[k], z = mp.e23[k];
+        const float cx = mp.cost[x], cy = mp.cost[y], cz = mp.cost[z];
+        const float nx = (float)(mp.inc_off[x + 1] - mp.inc_off[x]);
+        const float ny = (float)(mp.inc_off[y + 1] - mp.inc_off[y]);
+        const float nz = (float)(mp.inc_off[z + 1] - mp.inc_off[z]);
+        float t12 = __fadd_rn(mp.c12[k], __fdiv_rn(cx, nx));
+        float t13 = __fadd_rn(mp.c13[k], __fdiv_rn(cy, ny));
+        float t23 = __fadd_rn(mp.c23[k], __fdiv_rn(cz, nz));
+        float e12 = 0.0f, e13 = 0.0f, e23 = 0.0f;
+        {
+            float mm = min_marginal(t12, t13, t23);
+            t12 = sub_scaled(t12, third, mm);
+            e12 = add_scaled(e12, third, mm);
+        }
+        {
+            float mm = min_marginal(t13, t12, t23);
+            t13 = sub_scaled(t13, half, mm);
+            e13 = add_scaled(e13, half, mm);
+        }
+        {
+            float mm = min_marginal(t23, t12, t13);
+            t23 = __fsub_rn(t23, mm);
+            e23 = __fadd_rn(e23, mm);
+        }
+        {
+            float mm = min_marginal(t12, t13, t23);
+            t12 = sub_scaled(t12, half, mm);
+            e12 = add_scaled(e12, half, mm);
+        }
+        {
+            float mm = min_marginal(t13, t12, t23);
+            t13 = __fsub_rn(t13, mm);
+            e13 = __fadd_rn(e13, mm);
+        }
+        {
+            float mm = min_marginal(t12, t13, t23);
+            t12 = __fsub_rn(t12, mm);
+            e12 = __fadd_rn(e12, mm);
+        }
+        mp.c12[k] = t12;
+        mp.c13[k] = t13;
+        mp.c23[k] = t23;
+        mp.diff[3 * k] = e12;
+        mp.diff[3 * k + 1] = e13;
+        mp.diff[3 * k + 2] = e23;
+    }
+    t.sync();
+    // covered edges: c = 0 + RSUM(messages); long lists by a warp
+    for (int64_t e = t.rank(); e < mp.E; e += t.size()) {
+        const int32_t s = mp.inc_off[e], n = mp.inc_off[e + 1] - s;
+        if (n == 0 || n > 32) continue;
+        mp.cost[e] = __fadd_rn(0.0f, rsum_serial(n, [&](int k) { return mp.diff[mp.inc[s + k]]; }));
+    }
+    for (int64_t e = team_warp(t); e < mp.E; e += team_nwarps(t)) {
+        const int32_t s = mp.inc_off[e], n = mp.inc_off[e + 1] - s;
+        if (n <= 32) continue;
+        float v = rsum_warp(n, [&](int64_t k) { return mp.diff[mp.inc[s + k]]; });
+        if (lane_id() == 0) mp.cost[e] = __fadd_rn(0.0f, v);
+    }
+    t.sync();
+}
+
+// dual_update_cycle_length (src/dual_solver.cu:7-35).  On success the graph
+// in the top slot is replaced by the reparametrised one.
+template <class Team>
+__device__ double dual_update_cycle_length(const Team &t, Scratch &sc, char *sm, Graph &A, int c, int num_iter,
+                                           float tri_factor, float tol, int64_t *num_tri, bool *failed)
+{
+    uint64_t m = sc.arena.mark();
+    TriBuf tb;
+    conflicted_cycles(t, sc, sm, A, c, tri_factor, tol, tb);
+    *failed = !sc.arena.ok();
+    if (*failed) {
+        sc.arena.release(m);
+        return 0.0;
+    }
+    *num_tri = tb.count;
+    if (tb.count == 0) {
+        sc.arena.release(m);
+        return graph_lb(t, sc, A);
+    }
+    Mp mp;
+    if (!mp_build(t, sc, sm, A, tb, mp)) {
+        *failed = true;
+        sc.arena.release(m);
+        return 0.0;
+    }
+    double prev = 0.0;
+    for (int it = 0; it < num_iter; ++it) {
+        double lb = mp_lower_bound(t, sc, mp);
+        if (it > 0 && (lb - prev) < 1e-3) break;
+        mp_iteration(t, mp);
+        prev = lb;
+    }
+    const double fin = mp_lower_bound(t, sc, mp);
+    Graph g;
+    g.row = mp.row;
+    g.col = mp.col;
+    g.cost = mp.cost;
+    g.n = mp.E;
+    graph_set_dims(t, sc, sm, g);
+    Graph ng = graph_commit(t, sc, g);
+    *failed = !sc.arena.ok();
+    if (!*failed) A = ng;
+    sc.arena.release(m);
+    return fin;
+}
+
+// dual_solver (src/dual_solver.cu:37-63); an arena overflow plays the role of
+// the reference's bad_alloc: the trivial bound of the current graph is
+// returned and the graph keeps its last committed state.
+template <class Team>
+__device__ double dual_solver(const Team &t, Scratch &sc, char *sm, Graph &A, int max_len, int num_iter,
+                              float tri_factor, int num_outer, float tol, int64_t *num_tri_last, int *oom)
+{
+    if (num_tri_last) *num_tri_last = 0;
+    if (max_len < 3 || num_iter == 0 || num_outer == 0) return graph_lb(t, sc, A);
+    double prev = 0.0, fin = 0.0;
+    int64_t nt = 0;
+    for (int o = 0; o < num_outer; ++o) {
+        for (int c = 3; c <= max_len; ++c) {
+            bool failed = false;
+            fin = dual_update_cycle_length(t, sc, sm, A, c, num_iter, tri_factor, tol, &nt, &failed);
+            if (failed) {
+                sc.arena.failed = 0;
+                if (oom) *oom = 1;
+                return graph_lb(t, sc, A);
+            }
+        }
+        if (nt == 0 || (o > 0 && (fin - prev) < 1e-3)) break;
+        prev = fin;
+    }
+    if (num_tri_last) *num_tri_last = nt;
+    return fin;
+}
+
+}  // namespace rama
