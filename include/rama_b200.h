@@ -72,6 +72,7 @@ typedef struct {
     int64_t edges_after_dual;
     int64_t workspace_peak;  /* bytes */
     double device_ms;        /* kernel time of the solve (CUDA events) */
+    double alg_bytes;        /* algorithmic bytes of the solve */
 } rama_stats;
 
 /*

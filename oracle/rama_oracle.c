@@ -280,17 +280,6 @@ orc_graph *orc_graph_from_sorted(int64_t n, const int32_t *row, const int32_t *c
     return g;
 }
 
-static orc_graph *graph_clone(const orc_graph *A)
-{
-    orc_graph *g = graph_alloc(A->n);
-    memcpy(g->row, A->row, sizeof(int32_t) * (size_t)A->n);
-    memcpy(g->col, A->col, sizeof(int32_t) * (size_t)A->n);
-    memcpy(g->cost, A->cost, sizeof(float) * (size_t)A->n);
-    g->rows = A->rows;
-    g->cols = A->cols;
-    return g;
-}
-
 void orc_graph_info(const orc_graph *g, int64_t *n, int32_t *rows, int32_t *cols)
 {
     if (n) *n = g->n;

@@ -54,6 +54,7 @@ class RamaStats(C.Structure):
         ("edges_after_dual", C.c_int64),
         ("workspace_peak", C.c_int64),
         ("device_ms", C.c_double),
+        ("alg_bytes", C.c_double),
     ]
 
 

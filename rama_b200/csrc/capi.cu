@@ -49,6 +49,7 @@ __device__ __forceinline__ Scratch make_scratch(char *base, uint64_t bytes)
     sc.part[0] = base;
     sc.part[1] = base + PART_BYTES;
     sc.parity = 0;
+    sc.alg_bytes = 0.0;
     sc.arena.base = base;
     sc.arena.cap = bytes - 256;
     sc.arena.lo = 2 * PART_BYTES;
@@ -324,6 +325,8 @@ struct rama_context {
     int device = 0;
     int sms = 0;
     int grid_ctas = 0;  // co-resident CTAs of k_solve_grid
+    int step_ctas = 0;  // ... of k_step_grid
+    int obj_ctas = 0;   // ... of k_objective
     int cta_per_sm = 0;
     char *ws = nullptr;
     uint64_t ws_bytes = 0;
@@ -341,6 +344,10 @@ struct rama_context {
     int64_t tl_labels = 0;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     rama_stats stats{};
+    // device staging of rama_solve_host (grown on demand, reused)
+    int32_t *io_i = nullptr, *io_j = nullptr, *io_l = nullptr;
+    float *io_c = nullptr;
+    int64_t io_edges = 0, io_labels = 0;
 };
 
 namespace {
@@ -414,7 +421,7 @@ int solve_one(rama_context *h, const int32_t *d_i, const int32_t *d_j, const flo
     int32_t *tl = nullptr;
     int64_t tl_cap = 0;
     if (opts->dump_timeline) {
-        tl_cap = std::min<int64_t>((int64_t)cap * 64, (int64_t)1 << 28);
+        tl_cap = std::min<int64_t>(std::min<int64_t>(cap, (int64_t)1 << 22) * 64, (int64_t)1 << 28);
         if (h->tl_cap < tl_cap) {
             if (h->d_timeline) cudaFree(h->d_timeline);
             CU(cudaMalloc(&h->d_timeline, sizeof(int32_t) * (size_t)tl_cap));
@@ -465,6 +472,7 @@ int solve_one(rama_context *h, const int32_t *d_i, const int32_t *d_j, const flo
         h->stats.edges_after_dual = ho.edges_after_dual;
         h->stats.workspace_peak = ho.arena_peak;
         h->stats.device_ms = ms;
+        h->stats.alg_bytes = ho.alg_bytes;
         if (opts->dump_timeline && ho.timeline_rounds > 0) {
             h->tl_rounds = ho.timeline_rounds;
             h->tl_labels = ho.num_labels;
@@ -550,6 +558,10 @@ int rama_create(int device, uint64_t workspace_bytes, rama_handle *out)
         return fail(RAMA_ERR_CUDA, "solver kernel does not fit on an SM");
     }
     h->grid_ctas = per_sm * h->sms;
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_grid, THREADS, SMEM));
+    h->step_ctas = std::max(1, per_sm) * h->sms;
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_objective, THREADS, SMEM));
+    h->obj_ctas = std::max(1, per_sm) * h->sms;
     int per_sm_cta = 0;
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_cta, k_solve_cta, THREADS, SMEM));
     h->cta_per_sm = std::max(1, per_sm_cta);
@@ -573,6 +585,10 @@ void rama_destroy(rama_handle h)
     cudaFree(h->d_step);
     cudaFree(h->d_scalar);
     cudaFree(h->d_timeline);
+    cudaFree(h->io_i);
+    cudaFree(h->io_j);
+    cudaFree(h->io_c);
+    cudaFree(h->io_l);
     cudaEventDestroy(h->ev0);
     cudaEventDestroy(h->ev1);
     delete h;
@@ -597,13 +613,28 @@ int rama_solve_host(rama_handle h, const int32_t *i, const int32_t *j, const flo
     int32_t mx = -1;
     for (int64_t e = 0; e < n; ++e) mx = std::max(mx, std::max(i[e], j[e]));
     const int64_t cap = (int64_t)mx + 1;
-    int32_t *di = nullptr, *dj = nullptr, *dl = nullptr;
-    float *dc = nullptr;
-    const size_t nb = sizeof(int32_t) * (size_t)std::max<int64_t>(n, 1);
-    CU(cudaMalloc(&di, nb));
-    CU(cudaMalloc(&dj, nb));
-    CU(cudaMalloc(&dc, nb));
-    CU(cudaMalloc(&dl, sizeof(int32_t) * (size_t)std::max<int64_t>(cap, 1)));
+    if (h->io_edges < std::max<int64_t>(n, 1)) {
+        cudaFree(h->io_i);
+        cudaFree(h->io_j);
+        cudaFree(h->io_c);
+        h->io_i = h->io_j = nullptr;
+        h->io_c = nullptr;
+        h->io_edges = 0;
+        const size_t nb = sizeof(int32_t) * (size_t)std::max<int64_t>(n, 1);
+        CU(cudaMalloc(&h->io_i, nb));
+        CU(cudaMalloc(&h->io_j, nb));
+        CU(cudaMalloc(&h->io_c, nb));
+        h->io_edges = std::max<int64_t>(n, 1);
+    }
+    if (h->io_labels < std::max<int64_t>(cap, 1)) {
+        cudaFree(h->io_l);
+        h->io_l = nullptr;
+        h->io_labels = 0;
+        CU(cudaMalloc(&h->io_l, sizeof(int32_t) * (size_t)std::max<int64_t>(cap, 1)));
+        h->io_labels = std::max<int64_t>(cap, 1);
+    }
+    int32_t *di = h->io_i, *dj = h->io_j, *dl = h->io_l;
+    float *dc = h->io_c;
     cudaStream_t st = nullptr;
     CU(cudaMemcpyAsync(di, i, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
     CU(cudaMemcpyAsync(dj, j, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
@@ -618,10 +649,6 @@ int rama_solve_host(rama_handle h, const int32_t *i, const int32_t *j, const flo
         if (num_labels) *num_labels = nl;
         if (solve_ms) *solve_ms = h->stats.device_ms;
     }
-    cudaFree(di);
-    cudaFree(dj);
-    cudaFree(dc);
-    cudaFree(dl);
     return rc;
 }
 
@@ -725,7 +752,7 @@ int rama_objective(rama_handle h, const int32_t *d_i, const int32_t *d_j, const 
     if (rc) return rc;
     void *args[] = {(void *)&d_i, (void *)&d_j, (void *)&d_costs, (void *)&n, (void *)&d_labels,
                     (void *)&h->d_scalar, (void *)&h->ws, (void *)&h->ws_bytes};
-    CU(cudaLaunchCooperativeKernel((void *)k_objective, dim3(h->grid_ctas), dim3(THREADS), args, SMEM, st));
+    CU(cudaLaunchCooperativeKernel((void *)k_objective, dim3(h->obj_ctas), dim3(THREADS), args, SMEM, st));
     CU(cudaMemcpyAsync(obj, h->d_scalar, sizeof(double), cudaMemcpyDeviceToHost, st));
     CU(cudaStreamSynchronize(st));
     return RAMA_OK;
@@ -743,7 +770,7 @@ int rama_step(rama_handle h, rama_step_args *a, void *stream)
     CU(cudaMemcpyAsync(h->d_step, a, sizeof(rama_step_args), cudaMemcpyHostToDevice, st));
     if (a->team == 2) {
         void *args[] = {(void *)&h->d_step, (void *)&h->ws, (void *)&h->ws_bytes};
-        CU(cudaLaunchCooperativeKernel((void *)k_step_grid, dim3(h->grid_ctas), dim3(THREADS), args, SMEM, st));
+        CU(cudaLaunchCooperativeKernel((void *)k_step_grid, dim3(h->step_ctas), dim3(THREADS), args, SMEM, st));
     } else {
         k_step_cta<<<1, THREADS, SMEM, st>>>(h->d_step, h->ws, h->ws_bytes);
         CU(cudaGetLastError());

@@ -258,6 +258,7 @@ __device__ void conflicted_cycles(const Team &t, Scratch &sc, char *sm, const Gr
             });
     }
     tb.num = tb.count < tb.budget ? tb.count : tb.budget;
+    sc.alg_bytes += 12.0 * (double)A.n + 8.0 * (double)R + 4.0 * (double)C.m2 + 12.0 * (double)tb.num;
 }
 
 }  // namespace rama

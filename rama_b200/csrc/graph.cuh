@@ -108,6 +108,7 @@ __device__ Graph graph_from_edges(const Team &t, Scratch &sc, char *sm, const in
     graph_set_dims(t, sc, sm, g);
     Graph r = graph_commit(t, sc, g);
     sc.arena.release(m);
+    sc.alg_bytes += 24.0 * (double)n;
     return r;
 }
 
@@ -192,7 +193,59 @@ __device__ Graph graph_contract(const Team &t, Scratch &sc, char *sm, const Grap
     h.cols = g.cols;
     Graph res = graph_commit(t, sc, h);
     sc.arena.release(m);
+    sc.alg_bytes += 20.0 * (double)n + 12.0 * (double)nruns;
     return res;
+}
+
+// compute_sanitized_graph (include/rama_utils.h:429-466): drop duplicate
+// edges (the first occurrence in stable (min,max) order survives), then
+// renumber the nodes that have edges to 0..k-1.  Outputs live in the
+// temporaries; idmap (size = max id + 1) maps original ids to new ones.
+template <class Team>
+__device__ int64_t sanitize_edges(const Team &t, Scratch &sc, char *sm, const int32_t *I, const int32_t *J,
+                                  const float *Cc, int64_t n, int32_t *&si, int32_t *&sj, float *&sw, int32_t *&idmap,
+                                  int32_t &idsize)
+{
+    int32_t mx = team_max<Team, int32_t>(t, sc, sm, n, 0, [&](int64_t e) { return I[e] > J[e] ? I[e] : J[e]; });
+    idsize = mx + 1;
+    const int nb = bits_for((uint64_t)mx);
+    si = sc.arena.take<int32_t>(n + 1);
+    sj = sc.arena.take<int32_t>(n + 1);
+    sw = sc.arena.take<float>(n + 1);
+    idmap = sc.arena.take<int32_t>((int64_t)idsize + 1);
+    uint64_t m = sc.arena.mark();
+    uint64_t *k1 = sc.arena.take<uint64_t>(n + 1), *k2 = sc.arena.take<uint64_t>(n + 1);
+    float *v1 = sc.arena.take<float>(n + 1), *v2 = sc.arena.take<float>(n + 1);
+    if (!sc.arena.ok()) return 0;
+    for (int64_t e = t.rank(); e < n; e += t.size()) {
+        int32_t a = I[e], b = J[e];
+        k1[e] = pack_key(a < b ? a : b, a < b ? b : a, nb);
+        v1[e] = Cc[e];
+    }
+    for (int64_t v = t.rank(); v < idsize; v += t.size()) idmap[v] = 0;
+    t.sync();
+    team_sort_pairs(t, sc, sm, k1, v1, k2, v2, n, 2 * nb);
+    const uint64_t mask = (nb == 0) ? 0 : ((uint64_t(1) << nb) - 1);
+    const int64_t u = team_compact(
+        t, sc, sm, n, [&](int64_t k) { return k == 0 || k1[k] != k1[k - 1]; },
+        [&](int64_t k, int64_t p) {
+            int32_t a = (int32_t)(k1[k] >> nb), b = (int32_t)(k1[k] & mask);
+            si[p] = a;
+            sj[p] = b;
+            sw[p] = v1[k];
+            idmap[a] = 1;
+            idmap[b] = 1;
+        });
+    team_scan<Team, int64_t>(
+        t, sc, sm, idsize, [&](int64_t v) -> int64_t { return idmap[v]; },
+        [&](int64_t v, int64_t pre, int64_t) { idmap[v] = (int32_t)pre; });
+    for (int64_t e = t.rank(); e < u; e += t.size()) {
+        si[e] = idmap[si[e]];
+        sj[e] = idmap[sj[e]];
+    }
+    t.sync();
+    sc.arena.release(m);
+    return u;
 }
 
 // Stable contraction WITHOUT diagonal removal (the raw contract_cuda result,

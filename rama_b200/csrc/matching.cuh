@@ -69,6 +69,7 @@ __device__ int32_t matching_contraction_map(const Team &t, Scratch &sc, char *sm
                 }
             }
             t.sync();
+            sc.alg_bytes += 12.0 * (double)C.m2 + 16.0 * (double)M;
             int32_t cur = team_sum<Team, int32_t>(t, sc, sm, M, [&](int64_t v) { return matched[v]; });
             float rel = (float)(cur - prev) / ((float)prev + 1.0f);
             prev = cur;

@@ -311,8 +311,10 @@ __device__ double dual_update_cycle_length(const Team &t, Scratch &sc, char *sm,
     double prev = 0.0;
     for (int it = 0; it < num_iter; ++it) {
         double lb = mp_lower_bound(t, sc, mp);
+        sc.alg_bytes += 4.0 * (double)mp.E + 12.0 * (double)mp.T;
         if (it > 0 && (lb - prev) < 1e-3) break;
         mp_iteration(t, mp);
+        sc.alg_bytes += 84.0 * (double)mp.T + 12.0 * (double)mp.E;
         prev = lb;
     }
     const double fin = mp_lower_bound(t, sc, mp);

@@ -24,6 +24,7 @@ struct Scratch {
     Arena arena;
     char *part[2];  // each >= 16 * (nblocks + 2) bytes
     int parity;
+    double alg_bytes;  // algorithmic bytes of the work done (team-uniform tally)
     __device__ __forceinline__ char *next_part()
     {
         parity ^= 1;

@@ -45,6 +45,7 @@ struct Instance {
     int64_t triangles_initial;
     int64_t arena_peak;
     int64_t edges_after_dual;
+    double alg_bytes;
 };
 
 __device__ __forceinline__ uint64_t global_ns()
@@ -74,10 +75,22 @@ __device__ void solve_instance(const Team &t, char *sm, Scratch sc, const Option
     });
     if (!sc.arena.ok()) status |= ERR_ARENA;
     if (bad_in) status |= ERR_INVALID_ARG;
+    int32_t *idmap = nullptr;
+    int32_t idsize = 0;
+    int64_t nin = n;
+    if (status == ERR_NONE && n > 0 && o.sanitize_graph) {
+        int32_t *si, *sj;
+        float *sw;
+        nin = sanitize_edges(t, sc, sm, I, J, Cc, n, si, sj, sw, idmap, idsize);
+        I = si;
+        J = sj;
+        Cc = sw;
+        if (!sc.arena.ok()) status |= ERR_ARENA;
+    }
     if (status == ERR_NONE && n > 0) {
         uint64_t t0 = 0;
         if (t.rank() == 0) slot[0] = global_ns();
-        Graph A = graph_from_edges(t, sc, sm, I, J, Cc, n);
+        Graph A = graph_from_edges(t, sc, sm, I, J, Cc, nin);
         t0 = uread(&slot[0]);
         if (!sc.arena.ok()) status |= ERR_ARENA;
         if (status == ERR_NONE) {
@@ -148,7 +161,19 @@ __device__ void solve_instance(const Team &t, char *sm, Scratch sc, const Option
                         if ((int64_t)((now - t0) / 1000000000ull) > (int64_t)o.max_time_sec) break;
                     }
                 }
-                if (status == ERR_NONE) {
+                if (status == ERR_NONE && idmap) {
+                    // desanitize_node_labels (include/rama_utils.h:468-493): -1 for ids without edges
+                    if (idsize > io->labels_cap)
+                        status |= ERR_INVALID_ARG;
+                    else {
+                        for (int64_t v = t.rank(); v < idsize; v += t.size()) {
+                            int32_t cur = idmap[v];
+                            bool present = (v == idsize - 1) || cur != idmap[v + 1];
+                            io->labels[v] = present ? nm[cur] : -1;
+                        }
+                        num_labels = idsize;
+                    }
+                } else if (status == ERR_NONE) {
                     if (N0 > io->labels_cap)
                         status |= ERR_INVALID_ARG;
                     else {
@@ -172,6 +197,7 @@ __device__ void solve_instance(const Team &t, char *sm, Scratch sc, const Option
         io->triangles_initial = ntri;
         io->arena_peak = (int64_t)sc.arena.peak;
         io->edges_after_dual = eafter;
+        io->alg_bytes = sc.alg_bytes;
     }
 }
 

@@ -319,25 +319,35 @@ __device__ bool forest_root(const Team &t, Scratch &sc, char *sm, Forest &F)
     return true;
 }
 
+// Walks v1 and v2 up to their meeting point in the rooted forest; la / lb =
+// edges walked on each side.  Returns false if the walk leaves the forest
+// (an unreached vertex or different trees), never reading outside par[].
+__device__ __forceinline__ bool forest_meet(const Forest &F, int32_t a, int32_t b, int32_t &la, int32_t &lb)
+{
+    la = lb = 0;
+    for (int32_t s = 0; s <= F.nn && a >= 0 && b >= 0 && F.dep[a] > F.dep[b]; ++s) {
+        a = F.par[a];
+        ++la;
+    }
+    for (int32_t s = 0; s <= F.nn && a >= 0 && b >= 0 && F.dep[b] > F.dep[a]; ++s) {
+        b = F.par[b];
+        ++lb;
+    }
+    for (int32_t s = 0; s <= F.nn && a >= 0 && b >= 0 && a != b; ++s) {
+        a = F.par[a];
+        b = F.par[b];
+        ++la;
+        ++lb;
+    }
+    return a >= 0 && b >= 0 && a == b;
+}
+
 template <class Team>
 __device__ int32_t forest_path_lengths(const Team &t, Scratch &sc, char *sm, Forest &F)
 {
     for (int64_t k = t.rank(); k < F.R; k += t.size()) {
-        int32_t a = F.rr[k], b = F.rc[k], L = 0;
-        while (F.dep[a] > F.dep[b]) {
-            a = F.par[a];
-            ++L;
-        }
-        while (F.dep[b] > F.dep[a]) {
-            b = F.par[b];
-            ++L;
-        }
-        while (a != b) {
-            a = F.par[a];
-            b = F.par[b];
-            L += 2;
-        }
-        F.plen[k] = L;
+        int32_t la, lb;
+        F.plen[k] = forest_meet(F, F.rr[k], F.rc[k], la, lb) ? la + lb : 0x3fffffff;
     }
     t.sync();
     return team_min<Team, int32_t>(t, sc, sm, F.R, 0x7fffffff, [&](int64_t k) { return F.plen[k]; });
@@ -355,21 +365,8 @@ __device__ bool forest_resolve(const Team &t, Scratch &sc, char *sm, Forest &F, 
     for (int64_t k = t.rank(); k < F.R; k += t.size()) {
         if (F.plen[k] != s) continue;
         const int32_t v1 = F.rr[k], v2 = F.rc[k];
-        int32_t a = v1, b = v2, la = 0, lb = 0;
-        while (F.dep[a] > F.dep[b]) {
-            a = F.par[a];
-            ++la;
-        }
-        while (F.dep[b] > F.dep[a]) {
-            b = F.par[b];
-            ++lb;
-        }
-        while (a != b) {
-            a = F.par[a];
-            b = F.par[b];
-            ++la;
-            ++lb;
-        }
+        int32_t la = 0, lb = 0;
+        if (!forest_meet(F, v1, v2, la, lb)) continue;
         const int32_t L = la + lb;
         // row half: path[q], q in [0,dr); path[q] is v1's up edge q (q<la) or
         // v2's up edge L-1-q (q>=la)

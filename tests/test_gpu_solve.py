@@ -149,3 +149,21 @@ def test_cli(tmp_path, oracle):
     lines = [ln for ln in open(out).read().split("\n") if ln.strip()]
     seen = sorted(int(x) for ln in lines for x in ln.split())
     assert seen == list(range(100))
+
+
+def test_sanitize_graph_matches_oracle(solver, oracle):
+    """sanitize_graph: duplicate edges dropped (first survives), nodes without
+    edges get label -1 (include/rama_utils.h:429-493 of the reference)."""
+    rng = np.random.default_rng(17)
+    i, j, c = instances.random_graph(400, 4, seed=17)
+    i = (i * 3 + 2).astype(np.int32)  # gaps in the ids
+    j = (j * 3 + 2).astype(np.int32)
+    dup = rng.integers(0, len(c), size=40)
+    i = np.concatenate([i, j[dup]])  # duplicates, reversed orientation
+    j = np.concatenate([j, i[dup]])
+    c = np.concatenate([c, rng.normal(size=40).astype(np.float32)])
+    for mode in ("P", "PD"):
+        olab, olb, _ = oracle.solve(i, j, c, mode, sanitize_graph=1)
+        glab, glb, _ = solver.solve(i, j, c, mode=mode, sanitize_graph=1)
+        assert np.array_equal(glab, olab) and glb == olb
+        assert (glab[0] == -1) and (glab[1] == -1)
