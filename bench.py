@@ -41,6 +41,7 @@ CONFIGS = {
     "c2p": dict(desc="3-D grid 256x256x64 + long range (+-4 x/y, +-2 z), P", mode="P"),
     "c3": dict(desc="random geometric k-NN graph, 1M points, k=20, D (dual only)", mode="D"),
     "c4": dict(desc="512 Delaunay region-adjacency graphs, n log-uniform [500,20000], batched PD", mode="PD"),
+    "c2s": dict(desc="3-D grid 64x64x32 + long range (profiling-size C2), PD", mode="PD"),
 }
 
 
@@ -62,6 +63,8 @@ def make_instance(cfg):
         return I.grid3d_longrange()
     if cfg == "c3":
         return I.knn_rgg()
+    if cfg == "c2s":
+        return I.grid3d_longrange(64, 64, 32, seed=1002)
     raise ValueError(cfg)
 
 
@@ -71,8 +74,8 @@ def cpu_sample(cfg):
 
     if cfg in ("c2", "c2p"):
         return I.grid3d_longrange(128, 128, 64, seed=1002), "3-D grid 128x128x64 + long range, same generator"
-    if cfg == "c1":
-        return I.grid2d(), "full instance"
+    if cfg in ("c1", "c2s"):
+        return make_instance(cfg), "full instance"
     if cfg == "c3":
         return I.knn_rgg(50_000, 20, seed=1003), "k-NN graph, 50k points, k=20, same generator"
     if cfg == "c4":
@@ -186,7 +189,7 @@ def run_ours(args, rank, world, local):
     st = C.c_void_p(stream.cuda_stream)
 
     def one():
-        return s.solve_device(d_i, d_j, d_c, mode=mode, labels=labels, stream=st)
+        return s.solve_device(d_i, d_j, d_c, mode=mode, labels=labels, stream=st, team=args.team)
 
     for _ in range(args.warmup):
         one()
@@ -246,6 +249,7 @@ def run_ours(args, rank, world, local):
                    "l2": "input 12 B/edge x %d edges > 126 MB L2" % E},
         "solves_per_s": world * args.steps / (ms_max / 1e3),
         "objective": obj, "lower_bound": lbs[-1], "rounds": stats.rounds, "team": stats.team,
+        "phase_ms": {n: round(stats.phase_ms[k], 3) for k, n in enumerate(_lib.PHASES) if n != "-"},
         "e2e": {"value": world * E / e2e_s, "unit": "edges/s", "h2d_bytes_per_step": 12 * E,
                 "d2h_bytes_per_step": 4 * N + 8, "api": "rama_solve_host"},
         "gpu_launches": args.steps,
@@ -444,6 +448,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--team", type=int, default=0, help="0 auto, 1 one CTA, 2 cooperative grid")
     args = ap.parse_args()
     rank, world, local = dist_setup(args.gpus)
     if args.impl == "reference":

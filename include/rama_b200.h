@@ -73,6 +73,8 @@ typedef struct {
     int64_t workspace_peak;  /* bytes */
     double device_ms;        /* kernel time of the solve (CUDA events) */
     double alg_bytes;        /* algorithmic bytes of the solve */
+    double phase_ms[10];     /* time per phase: init, cycle search, MP build, MP iterations + bound,
+                                dual commit, matching, forest contraction set, contraction, other, - */
 } rama_stats;
 
 /*
@@ -113,6 +115,22 @@ int rama_get_timeline(rama_handle h, int32_t *out, int64_t cap, int32_t *rounds,
 int rama_solve_batch(rama_handle h, const int32_t *d_i, const int32_t *d_j, const float *d_costs,
                      const int64_t *edge_offsets, int32_t count, const rama_options *opts, int32_t *d_labels,
                      const int64_t *label_offsets, int64_t *num_labels, double *lbs, int32_t *status, void *stream);
+
+/*
+ * Asynchronous batch (continuous batching): rama_batch_launch enqueues a batch
+ * on `stream` and returns at once; rama_batch_poll returns 1 when it has
+ * finished (0 while running, negative on error); rama_batch_wait blocks,
+ * then fills the host result arrays.  opts holds 1 entry (shared) or `count`
+ * entries (per instance).  Each instance gets a workspace slice sized from
+ * its edge count (about 1 KiB per edge); the sum is the batch's footprint.
+ * One batch in flight per handle: a server keeps one handle per concurrent
+ * batch.  No counterpart in the reference (it solves one instance per call).
+ */
+int rama_batch_launch(rama_handle h, const int32_t *d_i, const int32_t *d_j, const float *d_costs,
+                      const int64_t *edge_offsets, int32_t count, const rama_options *opts, int32_t opts_count,
+                      int32_t *d_labels, const int64_t *label_offsets, void *stream);
+int rama_batch_poll(rama_handle h);
+int rama_batch_wait(rama_handle h, int64_t *num_labels, double *lbs, int32_t *status);
 
 int rama_get_stats(rama_handle h, rama_stats *out);
 const char *rama_last_error(void);

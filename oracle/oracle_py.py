@@ -45,6 +45,7 @@ class OrcStats(C.Structure):
         ("mst_rounds", C.c_int32),
         ("triangles_initial", C.c_int64),
         ("status", C.c_int32),
+        ("truncations", C.c_int32),
     ]
 
 

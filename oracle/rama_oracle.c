@@ -1104,6 +1104,9 @@ int orc_woc(const orc_graph *A, int32_t *map_out, int64_t *map_size, int32_t *nr
 /* ------------------------------------------------------------------------ */
 /* conflicted cycles (src/conflicted_cycles_cuda.cu:13-343)                  */
 /* ------------------------------------------------------------------------ */
+/* number of cycle searches whose budget overflowed since the last reset
+ * (reported per solve in orc_stats.truncations; single-threaded use) */
+static int32_t g_truncations = 0;
 typedef struct {
     int32_t *buf; /* 3*budget */
     int64_t budget, count;
@@ -1270,6 +1273,7 @@ int orc_conflicted_cycles(const orc_graph *A, int32_t max_len, float tri_factor,
         }
     }
     int64_t keep = T.count < budget ? T.count : budget;
+    if (T.count > budget) g_truncations++;
     if (keep > tri_cap) keep = tri_cap;
     memcpy(tri_out, T.buf, sizeof(int32_t) * (size_t)(3 * keep));
     *num_out = keep;
@@ -1776,6 +1780,7 @@ int orc_solve(int64_t n, const int32_t *i, const int32_t *j, const float *c, con
         orc_sanitize(n, ii, jj, cc, &n, ids_mapping, (int64_t)mx + 1, &ids_size);
     }
     double t0 = now_sec();
+    g_truncations = 0;
     orc_graph *A = orc_graph_from_edges(n, ii, jj, cc);
     free(ii);
     free(jj);
@@ -1845,6 +1850,7 @@ int orc_solve(int64_t n, const int32_t *i, const int32_t *j, const float *c, con
     free(node_mapping);
     orc_graph_free(A);
     st.status = rc;
+    st.truncations = g_truncations;
     if (stats) *stats = st;
     return rc;
 }

@@ -59,6 +59,7 @@ typedef struct {
     int32_t mst_rounds;
     int64_t triangles_initial; /* triangles of the initial dual (last cycle length) */
     int32_t status;
+    int32_t truncations;       /* cycle searches whose triangle budget overflowed */
 } orc_stats;
 
 /* status codes shared with the CUDA library */

@@ -55,7 +55,10 @@ class RamaStats(C.Structure):
         ("workspace_peak", C.c_int64),
         ("device_ms", C.c_double),
         ("alg_bytes", C.c_double),
+        ("phase_ms", C.c_double * 10),
     ]
+
+PHASES = ("init", "cycles", "mp_build", "mp_iter", "dual_commit", "matching", "woc", "contract", "other", "-")
 
 
 _P = C.c_void_p
@@ -83,7 +86,8 @@ class StepArgs(C.Structure):
 
 # every symbol include/rama_b200.h declares
 EXPORTS = ("rama_options_init", "rama_create", "rama_destroy", "rama_solve", "rama_solve_host", "rama_get_timeline",
-           "rama_solve_batch", "rama_get_stats", "rama_last_error", "rama_objective", "rama_step")
+           "rama_solve_batch", "rama_batch_launch", "rama_batch_poll", "rama_batch_wait", "rama_get_stats",
+           "rama_last_error", "rama_objective", "rama_step")
 
 _lib = None
 _lock = threading.Lock()
@@ -115,6 +119,9 @@ def load():
                                       C.POINTER(C.c_double), C.POINTER(C.c_double)]
         L.rama_get_timeline.argtypes = [P, P, i64, C.POINTER(i32), C.POINTER(i64)]
         L.rama_solve_batch.argtypes = [P, P, P, P, P, i32, C.POINTER(RamaOptions), P, P, P, P, P, P]
+        L.rama_batch_launch.argtypes = [P, P, P, P, P, i32, P, i32, P, P, P]
+        L.rama_batch_poll.argtypes = [P]
+        L.rama_batch_wait.argtypes = [P, P, P, P]
         L.rama_get_stats.argtypes = [P, C.POINTER(RamaStats)]
         L.rama_last_error.restype = C.c_char_p
         L.rama_objective.argtypes = [P, P, P, P, i64, P, C.POINTER(C.c_double), P]

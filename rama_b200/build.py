@@ -39,13 +39,25 @@ def _stale(target, sources):
 
 
 def build_lib(force=False, verbose=False):
+    """Compiles every csrc/*.cu to an object (in parallel) and links the .so."""
     srcs = glob.glob(os.path.join(HERE, "csrc", "*")) + [os.path.join(INCLUDE, "rama_b200.h")]
     if not force and not _stale(LIB, srcs):
         return LIB
-    cmd = [NVCC, *NVCC_FLAGS, "-shared", "-o", LIB + ".tmp", os.path.join(HERE, "csrc", "capi.cu")]
-    if verbose:
-        cmd.insert(1, "-Xptxas=-v")
-    subprocess.run(cmd, check=True)
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+    units = sorted(glob.glob(os.path.join(HERE, "csrc", "*.cu")))
+    procs, objs = [], []
+    for u in units:
+        o = os.path.join(objdir, os.path.basename(u)[:-3] + ".o")
+        objs.append(o)
+        cmd = [NVCC, *NVCC_FLAGS, "-c", "-o", o, u]
+        if verbose:
+            cmd.insert(1, "-Xptxas=-v")
+        procs.append(subprocess.Popen(cmd))
+    if any(p.wait() != 0 for p in procs):
+        raise RuntimeError("nvcc failed")
+    subprocess.run([NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB + ".tmp", *objs],
+                   check=True)
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

@@ -50,6 +50,8 @@ __device__ __forceinline__ Scratch make_scratch(char *base, uint64_t bytes)
     sc.part[1] = base + PART_BYTES;
     sc.parity = 0;
     sc.alg_bytes = 0.0;
+    sc.prof = nullptr;
+    sc.tlast = 0;
     sc.arena.base = base;
     sc.arena.cap = bytes - 256;
     sc.arena.lo = 2 * PART_BYTES;
@@ -60,13 +62,10 @@ __device__ __forceinline__ Scratch make_scratch(char *base, uint64_t bytes)
 }
 
 struct CtaLaunch {
-    Options opts;
     Instance *inst;
     const int32_t *order;
     int32_t count;
     int32_t *queue;
-    char *ws;
-    uint64_t ws_per_cta;
 };
 
 __global__ void __launch_bounds__(THREADS, 2) k_solve_cta(CtaLaunch L)
@@ -74,21 +73,20 @@ __global__ void __launch_bounds__(THREADS, 2) k_solve_cta(CtaLaunch L)
     extern __shared__ __align__(16) char sm[];
     __shared__ int next;
     BlockTeam t;
-    char *base = L.ws + (uint64_t)blockIdx.x * L.ws_per_cta;
     for (int guard = 0; guard < (1 << 30); ++guard) {
         if (threadIdx.x == 0) next = atomicAdd(L.queue, 1);
         __syncthreads();
         const int k = next;
         __syncthreads();
         if (k >= L.count) break;
-        Scratch sc = make_scratch(base, L.ws_per_cta);
-        solve_instance(t, sm, sc, L.opts, &L.inst[L.order[k]]);
+        Instance *io = &L.inst[L.order[k]];
+        Scratch sc = make_scratch(io->ws, io->ws_bytes);
+        solve_instance(t, sm, sc, io);
         __syncthreads();
     }
 }
 
 struct GridLaunch {
-    Options opts;
     Instance *inst;
     char *ws;
     uint64_t ws_bytes;
@@ -99,7 +97,7 @@ __global__ void __launch_bounds__(THREADS, 2) k_solve_grid(GridLaunch L)
     extern __shared__ __align__(16) char sm[];
     GridTeam t;
     Scratch sc = make_scratch(L.ws, L.ws_bytes);
-    solve_instance(t, sm, sc, L.opts, L.inst);
+    solve_instance(t, sm, sc, L.inst);
 }
 
 // ---------------------------------------------------------------------------
@@ -339,6 +337,7 @@ struct rama_context {
     double *d_scalar = nullptr;
     int32_t *d_timeline = nullptr;
     int64_t tl_cap = 0;
+    int64_t *d_prof = nullptr;
     std::vector<int32_t> timeline;
     int32_t tl_rounds = 0;
     int64_t tl_labels = 0;
@@ -348,6 +347,15 @@ struct rama_context {
     int32_t *io_i = nullptr, *io_j = nullptr, *io_l = nullptr;
     float *io_c = nullptr;
     int64_t io_edges = 0, io_labels = 0;
+    // asynchronous batch in flight
+    bool b_active = false;
+    int32_t b_count = 0;
+    cudaStream_t b_stream = nullptr;
+    Instance *b_host = nullptr;  // pinned: instance descriptors in, results out
+    int32_t b_host_cap = 0;
+    std::vector<Instance> b_in;
+    std::vector<int32_t> b_order;
+    cudaEvent_t ev_done = nullptr;
 };
 
 namespace {
@@ -389,18 +397,20 @@ int ensure_inst(rama_context *h, int32_t count)
 }
 
 uint64_t ws_estimate(int64_t n_edges) { return (uint64_t)n_edges * 1024ull + (64ull << 20); }
+// workspace slice of one instance of a batch
+uint64_t ws_slice(int64_t n_edges) { return ((uint64_t)n_edges * 1024ull + (1ull << 20) + 4095) & ~uint64_t(4095); }
 
 // Launches the solve of the instances already in h->d_inst.  team 1: CTAs.
-int launch_solve(rama_context *h, const Options &o, int32_t count, int team, cudaStream_t st, uint64_t ws_per_cta)
+int launch_solve(rama_context *h, int32_t count, int team, cudaStream_t st)
 {
     if (team == 2) {
-        GridLaunch L{o, h->d_inst, h->ws, h->ws_bytes};
+        GridLaunch L{h->d_inst, h->ws, h->ws_bytes};
         void *args[] = {&L};
         CU(cudaLaunchCooperativeKernel((void *)k_solve_grid, dim3(h->grid_ctas), dim3(THREADS), args, SMEM, st));
     } else {
-        const int ctas = std::max(1, std::min<int>(count, (int)(h->ws_bytes / ws_per_cta)));
+        const int ctas = std::max(1, std::min<int>(count, h->sms * h->cta_per_sm));
         CU(cudaMemsetAsync(h->d_queue, 0, sizeof(int32_t), st));
-        CtaLaunch L{o, h->d_inst, h->d_order, count, h->d_queue, h->ws, ws_per_cta};
+        CtaLaunch L{h->d_inst, h->d_order, count, h->d_queue};
         k_solve_cta<<<ctas, THREADS, SMEM, st>>>(L);
         CU(cudaGetLastError());
     }
@@ -434,6 +444,7 @@ int solve_one(rama_context *h, const int32_t *d_i, const int32_t *d_j, const flo
         rc = ensure_ws(h, need);
         if (rc) return rc;
         Instance hi{};
+        hi.opts = o;
         hi.i = d_i;
         hi.j = d_j;
         hi.c = d_c;
@@ -442,11 +453,15 @@ int solve_one(rama_context *h, const int32_t *d_i, const int32_t *d_j, const flo
         hi.labels_cap = cap;
         hi.timeline = tl;
         hi.timeline_cap = tl_cap;
+        hi.prof = h->d_prof;
+        hi.ws = h->ws;
+        hi.ws_bytes = h->ws_bytes;
+        CU(cudaMemsetAsync(h->d_prof, 0, sizeof(int64_t) * PH_COUNT, st));
         int32_t zero = 0;
         CU(cudaMemcpyAsync(h->d_inst, &hi, sizeof(Instance), cudaMemcpyHostToDevice, st));
         CU(cudaMemcpyAsync(h->d_order, &zero, sizeof(int32_t), cudaMemcpyHostToDevice, st));
         CU(cudaEventRecord(h->ev0, st));
-        rc = launch_solve(h, o, 1, team, st, h->ws_bytes);
+        rc = launch_solve(h, 1, team, st);
         if (rc) return rc;
         CU(cudaEventRecord(h->ev1, st));
         Instance ho{};
@@ -473,6 +488,11 @@ int solve_one(rama_context *h, const int32_t *d_i, const int32_t *d_j, const flo
         h->stats.workspace_peak = ho.arena_peak;
         h->stats.device_ms = ms;
         h->stats.alg_bytes = ho.alg_bytes;
+        {
+            int64_t pr[PH_COUNT];
+            CU(cudaMemcpy(pr, h->d_prof, sizeof(pr), cudaMemcpyDeviceToHost));
+            for (int k = 0; k < PH_COUNT && k < 10; ++k) h->stats.phase_ms[k] = 1e-6 * (double)pr[k];
+        }
         if (opts->dump_timeline && ho.timeline_rounds > 0) {
             h->tl_rounds = ho.timeline_rounds;
             h->tl_labels = ho.num_labels;
@@ -568,8 +588,10 @@ int rama_create(int device, uint64_t workspace_bytes, rama_handle *out)
     CU(cudaMalloc(&h->d_queue, sizeof(int32_t) * 4));
     CU(cudaMalloc(&h->d_step, sizeof(rama_step_args)));
     CU(cudaMalloc(&h->d_scalar, sizeof(double) * 4));
+    CU(cudaMalloc(&h->d_prof, sizeof(int64_t) * PH_COUNT));
     CU(cudaEventCreate(&h->ev0));
     CU(cudaEventCreate(&h->ev1));
+    CU(cudaEventCreateWithFlags(&h->ev_done, cudaEventDisableTiming));
     *out = h;
     return RAMA_OK;
 }
@@ -585,12 +607,15 @@ void rama_destroy(rama_handle h)
     cudaFree(h->d_step);
     cudaFree(h->d_scalar);
     cudaFree(h->d_timeline);
+    cudaFree(h->d_prof);
     cudaFree(h->io_i);
     cudaFree(h->io_j);
     cudaFree(h->io_c);
     cudaFree(h->io_l);
     cudaEventDestroy(h->ev0);
     cudaEventDestroy(h->ev1);
+    cudaEventDestroy(h->ev_done);
+    if (h->b_host) cudaFreeHost(h->b_host);
     delete h;
 }
 
@@ -664,75 +689,153 @@ int rama_get_timeline(rama_handle h, int32_t *out, int64_t cap, int32_t *rounds,
     return RAMA_OK;
 }
 
+int rama_batch_launch(rama_handle h, const int32_t *d_i, const int32_t *d_j, const float *d_costs,
+                      const int64_t *edge_offsets, int32_t count, const rama_options *opts, int32_t opts_count,
+                      int32_t *d_labels, const int64_t *label_offsets, void *stream)
+{
+    if (!h || !opts || count < 0 || !edge_offsets || !label_offsets || (opts_count != 1 && opts_count != count))
+        return fail(RAMA_ERR_INVALID_ARG, "bad arguments");
+    if (h->b_active) return fail(RAMA_ERR_INVALID_ARG, "a batch is already in flight on this handle");
+    CU(cudaSetDevice(h->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    h->b_count = count;
+    h->b_stream = st;
+    if (count == 0) {
+        h->b_active = true;
+        return RAMA_OK;
+    }
+    int rc = ensure_inst(h, count);
+    if (rc) return rc;
+    if (h->b_host_cap < count) {
+        if (h->b_host) cudaFreeHost(h->b_host);
+        h->b_host = nullptr;
+        h->b_host_cap = 0;
+        CU(cudaHostAlloc(&h->b_host, sizeof(Instance) * (size_t)count, cudaHostAllocDefault));
+        h->b_host_cap = count;
+    }
+    h->b_in.assign(count, Instance{});
+    h->b_order.resize(count);
+    for (int32_t k = 0; k < count; ++k) {
+        const int64_t a = edge_offsets[k], b = edge_offsets[k + 1];
+        Instance &x = h->b_in[k];
+        x.opts = to_opts(&opts[opts_count == 1 ? 0 : k]);
+        x.i = d_i + a;
+        x.j = d_j + a;
+        x.c = d_costs + a;
+        x.n = b - a;
+        x.labels = d_labels + label_offsets[k];
+        x.labels_cap = label_offsets[k + 1] - label_offsets[k];
+        h->b_order[k] = k;
+    }
+    std::stable_sort(h->b_order.begin(), h->b_order.end(),
+                     [&](int32_t x, int32_t y) { return h->b_in[x].n > h->b_in[y].n; });
+    // every instance owns a workspace slice sized from its edge count; their
+    // sum is the batch's device footprint
+    uint64_t total = 0;
+    for (int32_t k = 0; k < count; ++k) total += ws_slice(h->b_in[k].n);
+    rc = ensure_ws(h, total);
+    if (rc) return rc;
+    if (h->ws_bytes < total) return fail(RAMA_ERR_OOM, "workspace too small for the batch");
+    {
+        uint64_t off = 0;
+        for (int32_t k = 0; k < count; ++k) {
+            h->b_in[k].ws = h->ws + off;
+            h->b_in[k].ws_bytes = ws_slice(h->b_in[k].n);
+            off += h->b_in[k].ws_bytes;
+        }
+    }
+    std::memcpy(h->b_host, h->b_in.data(), sizeof(Instance) * (size_t)count);
+    CU(cudaMemcpyAsync(h->d_inst, h->b_host, sizeof(Instance) * count, cudaMemcpyHostToDevice, st));
+    CU(cudaMemcpyAsync(h->d_order, h->b_order.data(), sizeof(int32_t) * count, cudaMemcpyHostToDevice, st));
+    CU(cudaEventRecord(h->ev0, st));
+    rc = launch_solve(h, count, 1, st);
+    if (rc) return rc;
+    CU(cudaEventRecord(h->ev1, st));
+    CU(cudaMemcpyAsync(h->b_host, h->d_inst, sizeof(Instance) * count, cudaMemcpyDeviceToHost, st));
+    CU(cudaEventRecord(h->ev_done, st));
+    h->b_active = true;
+    return RAMA_OK;
+}
+
+int rama_batch_poll(rama_handle h)
+{
+    if (!h || !h->b_active) return fail(RAMA_ERR_INVALID_ARG, "no batch in flight");
+    if (h->b_count == 0) return 1;
+    cudaError_t e = cudaEventQuery(h->ev_done);
+    if (e == cudaSuccess) return 1;
+    if (e == cudaErrorNotReady) return 0;
+    return -fail(RAMA_ERR_CUDA, std::string("batch: ") + cudaGetErrorString(e));
+}
+
+int rama_batch_wait(rama_handle h, int64_t *num_labels, double *lbs, int32_t *status)
+{
+    if (!h || !h->b_active) return fail(RAMA_ERR_INVALID_ARG, "no batch in flight");
+    h->b_active = false;
+    const int32_t count = h->b_count;
+    if (count == 0) return RAMA_OK;
+    CU(cudaSetDevice(h->device));
+    CU(cudaEventSynchronize(h->ev_done));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+    std::vector<Instance> out(h->b_host, h->b_host + count);
+    // instances that ran out of workspace are solved again with twice the slice
+    for (int attempt = 0; attempt < 3; ++attempt) {
+        std::vector<int32_t> redo;
+        for (int32_t k = 0; k < count; ++k)
+            if (out[k].status & ERR_ARENA) redo.push_back(k);
+        if (redo.empty()) break;
+        uint64_t total = 0;
+        for (int32_t k : redo) total += h->b_in[k].ws_bytes * 2;
+        int rc = ensure_ws(h, total);
+        if (rc) return rc;
+        std::vector<int32_t> order(redo.size());
+        std::iota(order.begin(), order.end(), 0);
+        std::vector<Instance> sub(redo.size());
+        uint64_t off = 0;
+        for (size_t q = 0; q < redo.size(); ++q) {
+            Instance &x = h->b_in[redo[q]];
+            x.ws_bytes *= 2;
+            x.ws = h->ws + off;
+            off += x.ws_bytes;
+            if (off > h->ws_bytes) return fail(RAMA_ERR_OOM, "workspace exhausted");
+            sub[q] = x;
+        }
+        CU(cudaMemcpyAsync(h->d_inst, sub.data(), sizeof(Instance) * sub.size(), cudaMemcpyHostToDevice, h->b_stream));
+        CU(cudaMemcpyAsync(h->d_order, order.data(), sizeof(int32_t) * order.size(), cudaMemcpyHostToDevice,
+                           h->b_stream));
+        rc = launch_solve(h, (int32_t)sub.size(), 1, h->b_stream);
+        if (rc) return rc;
+        CU(cudaMemcpyAsync(sub.data(), h->d_inst, sizeof(Instance) * sub.size(), cudaMemcpyDeviceToHost, h->b_stream));
+        CU(cudaStreamSynchronize(h->b_stream));
+        for (size_t q = 0; q < redo.size(); ++q) out[redo[q]] = sub[q];
+    }
+    int worst = RAMA_OK;
+    int64_t peak = 0;
+    double alg = 0.0;
+    for (int32_t k = 0; k < count; ++k) {
+        if (num_labels) num_labels[k] = out[k].num_labels;
+        if (lbs) lbs[k] = out[k].lb;
+        if (status) status[k] = status_from_bits(out[k].status);
+        if (out[k].status && worst == RAMA_OK) worst = status_from_bits(out[k].status);
+        peak = std::max<int64_t>(peak, out[k].arena_peak);
+        alg += out[k].alg_bytes;
+    }
+    h->stats = rama_stats{};
+    h->stats.team = 1;
+    h->stats.workspace_peak = peak;
+    h->stats.device_ms = ms;
+    h->stats.alg_bytes = alg;
+    if (worst) return fail(worst, "at least one instance failed (see status)");
+    return RAMA_OK;
+}
+
 int rama_solve_batch(rama_handle h, const int32_t *d_i, const int32_t *d_j, const float *d_costs,
                      const int64_t *edge_offsets, int32_t count, const rama_options *opts, int32_t *d_labels,
                      const int64_t *label_offsets, int64_t *num_labels, double *lbs, int32_t *status, void *stream)
 {
-    if (!h || !opts || count < 0 || !edge_offsets || !label_offsets) return fail(RAMA_ERR_INVALID_ARG, "bad arguments");
-    if (count == 0) return RAMA_OK;
-    CU(cudaSetDevice(h->device));
-    cudaStream_t st = (cudaStream_t)stream;
-    int rc = ensure_inst(h, count);
+    int rc = rama_batch_launch(h, d_i, d_j, d_costs, edge_offsets, count, opts, 1, d_labels, label_offsets, stream);
     if (rc) return rc;
-    std::vector<Instance> hi(count);
-    std::vector<int32_t> order(count);
-    int64_t emax = 0;
-    for (int32_t k = 0; k < count; ++k) {
-        const int64_t a = edge_offsets[k], b = edge_offsets[k + 1];
-        hi[k] = Instance{};
-        hi[k].i = d_i + a;
-        hi[k].j = d_j + a;
-        hi[k].c = d_costs + a;
-        hi[k].n = b - a;
-        hi[k].labels = d_labels + label_offsets[k];
-        hi[k].labels_cap = label_offsets[k + 1] - label_offsets[k];
-        emax = std::max(emax, b - a);
-        order[k] = k;
-    }
-    std::stable_sort(order.begin(), order.end(),
-                     [&](int32_t x, int32_t y) { return hi[x].n > hi[y].n; });
-    Options o = to_opts(opts);
-    uint64_t per_cta = ws_estimate(emax);
-    per_cta = (per_cta + 4095) & ~uint64_t(4095);
-    const int ctas = std::min<int>(count, h->sms * h->cta_per_sm);
-    for (int attempt = 0; attempt < 4; ++attempt) {
-        rc = ensure_ws(h, per_cta * (uint64_t)ctas);
-        if (rc) return rc;
-        if (h->ws_bytes < per_cta) return fail(RAMA_ERR_OOM, "workspace too small for one instance");
-        CU(cudaMemcpyAsync(h->d_inst, hi.data(), sizeof(Instance) * count, cudaMemcpyHostToDevice, st));
-        CU(cudaMemcpyAsync(h->d_order, order.data(), sizeof(int32_t) * count, cudaMemcpyHostToDevice, st));
-        CU(cudaEventRecord(h->ev0, st));
-        rc = launch_solve(h, o, count, 1, st, per_cta);
-        if (rc) return rc;
-        CU(cudaEventRecord(h->ev1, st));
-        std::vector<Instance> ho(count);
-        CU(cudaMemcpyAsync(ho.data(), h->d_inst, sizeof(Instance) * count, cudaMemcpyDeviceToHost, st));
-        CU(cudaStreamSynchronize(st));
-        float ms = 0;
-        cudaEventElapsedTime(&ms, h->ev0, h->ev1);
-        bool arena = false;
-        for (auto &x : ho) arena |= (x.status & ERR_ARENA) != 0;
-        if (arena && attempt < 3) {
-            per_cta *= 2;
-            continue;
-        }
-        int worst = RAMA_OK;
-        int64_t peak = 0;
-        for (int32_t k = 0; k < count; ++k) {
-            if (num_labels) num_labels[k] = ho[k].num_labels;
-            if (lbs) lbs[k] = ho[k].lb;
-            if (status) status[k] = status_from_bits(ho[k].status);
-            if (ho[k].status && worst == RAMA_OK) worst = status_from_bits(ho[k].status);
-            peak = std::max<int64_t>(peak, ho[k].arena_peak);
-        }
-        h->stats = rama_stats{};
-        h->stats.team = 1;
-        h->stats.workspace_peak = peak;
-        h->stats.device_ms = ms;
-        if (worst) return fail(worst, "at least one instance failed (see status)");
-        return RAMA_OK;
-    }
-    return fail(RAMA_ERR_OOM, "solver workspace exhausted");
+    return rama_batch_wait(h, num_labels, lbs, status);
 }
 
 int rama_get_stats(rama_handle h, rama_stats *out)

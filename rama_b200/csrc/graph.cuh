@@ -334,6 +334,8 @@ __device__ Csr build_symmetric_csr(const Team &t, Scratch &sc, char *sm, const G
     uint64_t *k1 = sc.arena.take<uint64_t>(m + 1), *k2 = sc.arena.take<uint64_t>(m + 1);
     int32_t *v1 = sc.arena.take<int32_t>(m + 1), *v2 = sc.arena.take<int32_t>(m + 1);
     int32_t *infill = sc.arena.take<int32_t>((int64_t)nrows + 1);
+    int32_t *colstart = sc.arena.take<int32_t>((int64_t)nrows + 1);
+    int32_t *rowstart = sc.arena.take<int32_t>((int64_t)nrows + 1);
     if (!sc.arena.ok()) return C;
     // 2. degrees (in + out) and in-degrees (number of u<v entries per row)
     for (int64_t v = t.rank(); v <= nrows; v += t.size()) infill[v] = 0;
@@ -350,24 +352,23 @@ __device__ Csr build_symmetric_csr(const Team &t, Scratch &sc, char *sm, const G
     team_scan<Team, int64_t>(
         t, sc, sm, (int64_t)nrows, [&](int64_t v) -> int64_t { return deg[v]; },
         [&](int64_t v, int64_t pre, int64_t) { C.off[v] = (int32_t)pre; });
+    // first position of each column among the column-sorted kept edges, and
+    // of each row among the (row-sorted) kept edges
+    team_scan<Team, int64_t>(
+        t, sc, sm, (int64_t)nrows, [&](int64_t v) -> int64_t { return infill[v]; },
+        [&](int64_t v, int64_t pre, int64_t) { colstart[v] = (int32_t)pre; });
+    team_scan<Team, int64_t>(
+        t, sc, sm, (int64_t)nrows, [&](int64_t v) -> int64_t { return deg[v] - infill[v]; },
+        [&](int64_t v, int64_t pre, int64_t) { rowstart[v] = (int32_t)pre; });
     if (t.rank() == 0) C.off[nrows] = (int32_t)(2 * m);
     t.sync();
     // 3. stable sort of kept edges by column -> reverse entries in increasing row order
     team_sort_pairs(t, sc, sm, k1, v1, k2, v2, m, bits_for((uint64_t)(nrows > 0 ? nrows : 1)));
     for (int64_t q = t.rank(); q < m; q += t.size()) {
         int32_t c = (int32_t)k1[q];
-        // position inside the run: binary search for the run start
-        int64_t lo = 0, hi = q;
-        while (lo < hi) {
-            int64_t mid = (lo + hi) >> 1;
-            if ((int32_t)k1[mid] < c)
-                lo = mid + 1;
-            else
-                hi = mid;
-        }
         int64_t p = v1[q];
         int64_t e = kidx[p];
-        int64_t dst = (int64_t)C.off[c] + (q - lo);
+        int64_t dst = (int64_t)C.off[c] + (q - colstart[c]);
         C.adj[dst] = A.row[e];
         C.w[dst] = A.cost[e];
         if (with_eid) C.eid[dst] = (int32_t)p;
@@ -376,15 +377,7 @@ __device__ Csr build_symmetric_csr(const Team &t, Scratch &sc, char *sm, const G
     for (int64_t p = t.rank(); p < m; p += t.size()) {
         int64_t e = kidx[p];
         int32_t r = A.row[e];
-        int64_t lo = 0, hi = p;  // first kept index with row r
-        while (lo < hi) {
-            int64_t mid = (lo + hi) >> 1;
-            if (A.row[kidx[mid]] < r)
-                lo = mid + 1;
-            else
-                hi = mid;
-        }
-        int64_t dst = (int64_t)C.off[r] + infill[r] + (p - lo);
+        int64_t dst = (int64_t)C.off[r] + infill[r] + (p - rowstart[r]);
         C.adj[dst] = A.col[e];
         C.w[dst] = A.cost[e];
         if (with_eid) C.eid[dst] = (int32_t)p;

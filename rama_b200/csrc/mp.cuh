@@ -291,7 +291,9 @@ __device__ double dual_update_cycle_length(const Team &t, Scratch &sc, char *sm,
 {
     uint64_t m = sc.arena.mark();
     TriBuf tb;
+    prof_mark(t, sc, PH_OTHER);
     conflicted_cycles(t, sc, sm, A, c, tri_factor, tol, tb);
+    prof_mark(t, sc, PH_CYCLES);
     *failed = !sc.arena.ok();
     if (*failed) {
         sc.arena.release(m);
@@ -308,6 +310,7 @@ __device__ double dual_update_cycle_length(const Team &t, Scratch &sc, char *sm,
         sc.arena.release(m);
         return 0.0;
     }
+    prof_mark(t, sc, PH_MP_BUILD);
     double prev = 0.0;
     for (int it = 0; it < num_iter; ++it) {
         double lb = mp_lower_bound(t, sc, mp);
@@ -318,6 +321,7 @@ __device__ double dual_update_cycle_length(const Team &t, Scratch &sc, char *sm,
         prev = lb;
     }
     const double fin = mp_lower_bound(t, sc, mp);
+    prof_mark(t, sc, PH_MP_ITER);
     Graph g;
     g.row = mp.row;
     g.col = mp.col;
@@ -325,6 +329,7 @@ __device__ double dual_update_cycle_length(const Team &t, Scratch &sc, char *sm,
     g.n = mp.E;
     graph_set_dims(t, sc, sm, g);
     Graph ng = graph_commit(t, sc, g);
+    prof_mark(t, sc, PH_DUAL_COMMIT);
     *failed = !sc.arena.ok();
     if (!*failed) A = ng;
     sc.arena.release(m);

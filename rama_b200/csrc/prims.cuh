@@ -25,12 +25,47 @@ struct Scratch {
     char *part[2];  // each >= 16 * (nblocks + 2) bytes
     int parity;
     double alg_bytes;  // algorithmic bytes of the work done (team-uniform tally)
+    int64_t *prof;     // optional per-phase nanoseconds (leader only)
+    uint64_t tlast;
     __device__ __forceinline__ char *next_part()
     {
         parity ^= 1;
         return part[parity];
     }
 };
+
+// Phase timing: the team leader charges the time since the last mark to
+// `phase`.  Marks sit right after team syncs, so a phase's time is the span
+// in which the whole team worked on it.
+enum Phase : int {
+    PH_INIT = 0,
+    PH_CYCLES = 1,
+    PH_MP_BUILD = 2,
+    PH_MP_ITER = 3,
+    PH_DUAL_COMMIT = 4,
+    PH_MATCHING = 5,
+    PH_WOC = 6,
+    PH_CONTRACT = 7,
+    PH_OTHER = 8,
+    PH_COUNT = 10
+};
+
+__device__ __forceinline__ uint64_t prof_now()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+template <class Team>
+__device__ __forceinline__ void prof_mark(const Team &t, Scratch &sc, int phase)
+{
+    if (sc.prof && t.leader()) {
+        uint64_t now = prof_now();
+        sc.prof[phase] += (int64_t)(now - sc.tlast);
+        sc.tlast = now;
+    }
+}
 
 // ---------------------------------------------------------------------------
 // block-level helpers (all threads of the CTA must call)

@@ -26,6 +26,7 @@ struct Options {
 
 // One instance: inputs, outputs and statistics (device memory).
 struct Instance {
+    Options opts;
     const int32_t *i, *j;
     const float *c;
     int64_t n;
@@ -33,6 +34,9 @@ struct Instance {
     int64_t labels_cap;
     int32_t *timeline;       // optional: rounds x num_labels
     int64_t timeline_cap;    // entries
+    int64_t *prof;           // optional: PH_COUNT nanosecond counters
+    char *ws;                // workspace slice of this instance (CTA solves)
+    uint64_t ws_bytes;
     // outputs
     int64_t num_labels;
     double lb;
@@ -56,8 +60,11 @@ __device__ __forceinline__ uint64_t global_ns()
 }
 
 template <class Team>
-__device__ void solve_instance(const Team &t, char *sm, Scratch sc, const Options &o, Instance *io)
+__device__ void solve_instance(const Team &t, char *sm, Scratch sc, Instance *io)
 {
+    const Options o = io->opts;
+    sc.prof = io->prof;
+    if (sc.prof && t.leader()) sc.tlast = prof_now();
     const int64_t n = io->n;
     const int32_t *I = io->i, *J = io->j;
     const float *Cc = io->c;
@@ -91,6 +98,7 @@ __device__ void solve_instance(const Team &t, char *sm, Scratch sc, const Option
         uint64_t t0 = 0;
         if (t.rank() == 0) slot[0] = global_ns();
         Graph A = graph_from_edges(t, sc, sm, I, J, Cc, nin);
+        prof_mark(t, sc, PH_INIT);
         t0 = uread(&slot[0]);
         if (!sc.arena.ok()) status |= ERR_ARENA;
         if (status == ERR_NONE) {
@@ -118,10 +126,12 @@ __device__ void solve_instance(const Team &t, char *sm, Scratch sc, const Option
                     int werr = 0;
                     if (try_mm) {
                         nr = matching_contraction_map(t, sc, sm, A, o.mean_multiplier_mm, map, &msize);
+                        prof_mark(t, sc, PH_MATCHING);
                         ++mrounds;
                         if ((float)nr < (float)A.rows * o.matching_thresh_crossover_ratio) try_mm = false;
                     } else {
                         nr = woc_contraction_map(t, sc, sm, A, map, &msize, &werr);
+                        prof_mark(t, sc, PH_WOC);
                         ++wrounds;
                         status |= werr;
                     }
@@ -132,6 +142,7 @@ __device__ void solve_instance(const Team &t, char *sm, Scratch sc, const Option
                     if (nr == 0) break;
                     int bad = 0;
                     A = graph_contract(t, sc, sm, A, map, msize - 1, &bad);
+                    prof_mark(t, sc, PH_CONTRACT);
                     if (!sc.arena.ok()) {
                         status |= ERR_ARENA;
                         break;
@@ -146,6 +157,7 @@ __device__ void solve_instance(const Team &t, char *sm, Scratch sc, const Option
                         if (m < msize) nm[v] = map[m];
                     }
                     t.sync();
+                    prof_mark(t, sc, PH_OTHER);
                     ++rounds;
                     if (o.dump_timeline && io->timeline &&
                         (int64_t)(tl_rounds + 1) * N0 <= io->timeline_cap) {

@@ -167,3 +167,43 @@ def test_sanitize_graph_matches_oracle(solver, oracle):
         glab, glb, _ = solver.solve(i, j, c, mode=mode, sanitize_graph=1)
         assert np.array_equal(glab, olab) and glb == olb
         assert (glab[0] == -1) and (glab[1] == -1)
+
+
+def test_async_batch_mixed_modes(solver, oracle):
+    """rama_batch_launch with per-instance options; poll until done, then wait.
+    Every instance equals its single solve in its own mode."""
+    import ctypes as C
+
+    import torch
+
+    from rama_b200 import _lib
+
+    rng = np.random.default_rng(23)
+    insts = [instances.delaunay(int(n), rng) for n in (300, 80, 1500, 40, 600)]
+    modes = ["P", "PD", "D", "PD+", "PD"]
+    batch = instances.pack(insts)
+    d = [torch.from_numpy(np.ascontiguousarray(x)).cuda() for x in (batch.i, batch.j, batch.c)]
+    lo = np.zeros(batch.count + 1, np.int64)
+    lo[1:] = np.cumsum(batch.node_counts)
+    lab = torch.empty(int(lo[-1]), dtype=torch.int32, device="cuda")
+    opts = (_lib.RamaOptions * batch.count)(*[_lib.options(m) for m in modes])
+    eo = np.ascontiguousarray(batch.edge_offsets, np.int64)
+    L = _lib.load()
+    h = solver.handle.h
+    st = C.c_void_p(torch.cuda.current_stream().cuda_stream)
+    _lib.check(L.rama_batch_launch(h, d[0].data_ptr(), d[1].data_ptr(), d[2].data_ptr(), eo.ctypes.data, batch.count,
+                                   opts, batch.count, lab.data_ptr(), lo.ctypes.data, st))
+    for _ in range(100000):
+        r = L.rama_batch_poll(h)
+        if r != 0:
+            break
+    assert r >= 0
+    nl = np.zeros(batch.count, np.int64)
+    lbs = np.zeros(batch.count)
+    status = np.zeros(batch.count, np.int32)
+    _lib.check(L.rama_batch_wait(h, nl.ctypes.data, lbs.ctypes.data, status.ctypes.data))
+    out = lab.cpu().numpy()
+    for k, (i, j, c) in enumerate(insts):
+        olab, olb, _ = oracle.solve(i, j, c, modes[k])
+        assert lbs[k] == olb
+        assert np.array_equal(out[lo[k]:lo[k] + nl[k]], olab)
