@@ -132,6 +132,31 @@ int rama_batch_launch(rama_handle h, const int32_t *d_i, const int32_t *d_j, con
 int rama_batch_poll(rama_handle h);
 int rama_batch_wait(rama_handle h, int64_t *num_labels, double *lbs, int32_t *status);
 
+/*
+ * Solve one small instance without allocating any device memory.  For callers
+ * that must not call cudaMalloc: an application whose device memory is fully
+ * reserved by its own pool allocator, a latency-critical loop that cannot
+ * afford cudaMalloc's device-wide synchronisation, or a process with a fixed
+ * device-memory budget.  No counterpart in the reference.
+ *
+ * Same inputs, outputs and results as rama_solve (one CTA solves the
+ * instance), but the scratch memory is one fixed 32 MiB array inside the
+ * library, held on every GPU that loads it until the process exits.  Limits:
+ * at most RAMA_STATIC_MAX_EDGES edges and node ids below
+ * RAMA_STATIC_MAX_NODES; larger instances are rejected with
+ * RAMA_ERR_INVALID_ARG, and an instance whose solve needs more scratch than
+ * the array returns RAMA_ERR_OOM.  dump_timeline is ignored.
+ * The first call on a device looks up the array's device address; make that
+ * first call before any stream capture.  All calls share the one array: calls
+ * that overlap on the GPU (other streams or host threads) race and must be
+ * serialised by the caller.
+ */
+#define RAMA_STATIC_MAX_EDGES 30000
+#define RAMA_STATIC_MAX_NODES 65536
+int rama_solve_small_static(const int32_t *d_i, const int32_t *d_j, const float *d_costs, int64_t num_edges,
+                            const rama_options *opts, int32_t *d_labels, int64_t labels_cap, int64_t *num_labels,
+                            double *lb, void *stream);
+
 int rama_get_stats(rama_handle h, rama_stats *out);
 const char *rama_last_error(void);
 

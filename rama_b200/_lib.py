@@ -87,7 +87,7 @@ class StepArgs(C.Structure):
 # every symbol include/rama_b200.h declares
 EXPORTS = ("rama_options_init", "rama_create", "rama_destroy", "rama_solve", "rama_solve_host", "rama_get_timeline",
            "rama_solve_batch", "rama_batch_launch", "rama_batch_poll", "rama_batch_wait", "rama_get_stats",
-           "rama_last_error", "rama_objective", "rama_step")
+           "rama_last_error", "rama_objective", "rama_step", "rama_solve_small_static")
 
 _lib = None
 _lock = threading.Lock()
@@ -123,6 +123,8 @@ def load():
         L.rama_batch_poll.argtypes = [P]
         L.rama_batch_wait.argtypes = [P, P, P, P]
         L.rama_get_stats.argtypes = [P, C.POINTER(RamaStats)]
+        L.rama_solve_small_static.argtypes = [P, P, P, i64, C.POINTER(RamaOptions), P, i64, C.POINTER(i64),
+                                              C.POINTER(C.c_double), P]
         L.rama_last_error.restype = C.c_char_p
         L.rama_objective.argtypes = [P, P, P, P, i64, P, C.POINTER(C.c_double), P]
         L.rama_step.argtypes = [P, C.POINTER(StepArgs), P]

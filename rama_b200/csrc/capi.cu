@@ -319,6 +319,9 @@ Options to_opts(const rama_options *o)
 
 }  // namespace
 
+// error text for the entry points of other translation units (noalloc.cu)
+void rama_set_last_error(const std::string &msg) { g_err = msg; }
+
 struct rama_context {
     int device = 0;
     int sms = 0;
