@@ -19,8 +19,11 @@ struct Mp {
     float *diff;  // 3T
     int32_t *row, *col;
     float *cost;
+    float *share;      // E: cost / number of incident triangles (covered edges)
     int32_t *inc_off;  // E + 1
     int32_t *inc;      // 3T
+    int32_t *longe;    // edges with more than 32 incident triangles
+    int64_t nlong;
     int32_t rows, cols;
 };
 
@@ -167,6 +170,19 @@ __device__ bool mp_build(const Team &t, Scratch &sc, char *sm, const Graph &A, T
     }
     team_offsets(t, 3 * T, (int32_t)E, [&](int64_t k) { return (int32_t)qk[k]; }, mp.inc_off);
     sc.arena.release(ik);
+    // each covered edge's share of its cost, and the edges whose incoming
+    // messages a whole warp sums
+    mp.share = sc.arena.take<float>(E + 1);
+    mp.longe = sc.arena.take<int32_t>(E + 1);
+    if (!sc.arena.ok()) return false;
+    mp.nlong = team_compact(
+        t, sc, sm, E, [&](int64_t e) { return mp.inc_off[e + 1] - mp.inc_off[e] > 32; },
+        [&](int64_t e, int64_t p) { mp.longe[p] = (int32_t)e; });
+    for (int64_t e = t.rank(); e < E; e += t.size()) {
+        const int32_t n = mp.inc_off[e + 1] - mp.inc_off[e];
+        mp.share[e] = n > 0 ? __fdiv_rn(mp.cost[e], (float)n) : 0.0f;
+    }
+    t.sync();
     mp.rows = A.rows;
     mp.cols = A.cols;
     return true;
@@ -221,14 +237,9 @@ __device__ void mp_iteration(const Team &t, const Mp &mp)
 {
     const double third = 1.0 / 3.0, half = 1.0 / 2.0;
     for (int64_t k = t.rank(); k < mp.T; k += t.size()) {
-        const int32_t x = mp.e12[k], y = mp.e13[k], z = mp.e23[k];
-        const float cx = mp.cost[x], cy = mp.cost[y], cz = mp.cost[z];
-        const float nx = (float)(mp.inc_off[x + 1] - mp.inc_off[x]);
-        const float ny = (float)(mp.inc_off[y + 1] - mp.inc_off[y]);
-        const float nz = (float)(mp.inc_off[z + 1] - mp.inc_off[z]);
-        float t12 = __fadd_rn(mp.c12[k], __fdiv_rn(cx, nx));
-        float t13 = __fadd_rn(mp.c13[k], __fdiv_rn(cy, ny));
-        float t23 = __fadd_rn(mp.c23[k], __fdiv_rn(cz, nz));
+        float t12 = __fadd_rn(mp.c12[k], mp.share[mp.e12[k]]);
+        float t13 = __fadd_rn(mp.c13[k], mp.share[mp.e13[k]]);
+        float t23 = __fadd_rn(mp.c23[k], mp.share[mp.e23[k]]);
         float e12 = 0.0f, e13 = 0.0f, e23 = 0.0f;
         {
             float mm = min_marginal(t12, t13, t23);
@@ -272,13 +283,18 @@ __device__ void mp_iteration(const Team &t, const Mp &mp)
     for (int64_t e = t.rank(); e < mp.E; e += t.size()) {
         const int32_t s = mp.inc_off[e], n = mp.inc_off[e + 1] - s;
         if (n == 0 || n > 32) continue;
-        mp.cost[e] = __fadd_rn(0.0f, rsum_serial(n, [&](int k) { return mp.diff[mp.inc[s + k]]; }));
+        const float c = __fadd_rn(0.0f, rsum_serial(n, [&](int k) { return mp.diff[mp.inc[s + k]]; }));
+        mp.cost[e] = c;
+        mp.share[e] = __fdiv_rn(c, (float)n);
     }
-    for (int64_t e = team_warp(t); e < mp.E; e += team_nwarps(t)) {
+    for (int64_t q = team_warp(t); q < mp.nlong; q += team_nwarps(t)) {
+        const int32_t e = mp.longe[q];
         const int32_t s = mp.inc_off[e], n = mp.inc_off[e + 1] - s;
-        if (n <= 32) continue;
-        float v = rsum_warp(n, [&](int64_t k) { return mp.diff[mp.inc[s + k]]; });
-        if (lane_id() == 0) mp.cost[e] = __fadd_rn(0.0f, v);
+        const float c = __fadd_rn(0.0f, rsum_warp(n, [&](int64_t k) { return mp.diff[mp.inc[s + k]]; }));
+        if (lane_id() == 0) {
+            mp.cost[e] = c;
+            mp.share[e] = __fdiv_rn(c, (float)n);
+        }
     }
     t.sync();
 }

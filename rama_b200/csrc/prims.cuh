@@ -166,6 +166,23 @@ __device__ __forceinline__ void block_chunk(const Team &t, int64_t n, int64_t &l
 // ---------------------------------------------------------------------------
 // team reductions (integer / min / max): one team sync
 // ---------------------------------------------------------------------------
+
+// Combines the per-CTA partials part[0, nb) written before the last team
+// sync.  Every warp reads them with independent L2 loads (ld.global.cg: the
+// values come from other SMs, so L1 must not serve them) spread over its
+// lanes, then combines the lanes; the result is valid on every lane.  Only
+// for exact operations (integer sums, min, max), whose result does not depend
+// on the combination order.
+template <class T, class Op>
+__device__ __forceinline__ T warp_fold_parts(const T *part, int nb, T init, Op op)
+{
+    T r = init;
+    for (int b = lane_id(); b < nb; b += 32) r = op(r, __ldcg(part + b));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) r = op(r, __shfl_xor_sync(FULL, r, o));
+    return r;
+}
+
 template <class Team, class T, class Get>
 __device__ T team_sum(const Team &t, Scratch &sc, char *sm, int64_t n, Get get)
 {
@@ -175,9 +192,7 @@ __device__ T team_sum(const Team &t, Scratch &sc, char *sm, int64_t n, Get get)
     T *part = reinterpret_cast<T *>(sc.next_part());
     if (threadIdx.x == 0) part[t.block()] = s;
     t.sync();
-    T r = T(0);
-    for (int b = 0; b < t.nblocks(); ++b) r += uread(&part[b]);
-    return r;
+    return warp_fold_parts<T>(part, t.nblocks(), T(0), [](T a, T b) { return a + b; });
 }
 
 template <class Team, class T, class Get>
@@ -192,12 +207,7 @@ __device__ T team_max(const Team &t, Scratch &sc, char *sm, int64_t n, T init, G
     T *part = reinterpret_cast<T *>(sc.next_part());
     if (threadIdx.x == 0) part[t.block()] = s;
     t.sync();
-    T r = init;
-    for (int b = 0; b < t.nblocks(); ++b) {
-        T x = uread(&part[b]);
-        r = x > r ? x : r;
-    }
-    return r;
+    return warp_fold_parts<T>(part, t.nblocks(), init, [](T a, T b) { return b > a ? b : a; });
 }
 
 template <class Team, class T, class Get>
@@ -212,12 +222,7 @@ __device__ T team_min(const Team &t, Scratch &sc, char *sm, int64_t n, T init, G
     T *part = reinterpret_cast<T *>(sc.next_part());
     if (threadIdx.x == 0) part[t.block()] = s;
     t.sync();
-    T r = init;
-    for (int b = 0; b < t.nblocks(); ++b) {
-        T x = uread(&part[b]);
-        r = x < r ? x : r;
-    }
-    return r;
+    return warp_fold_parts<T>(part, t.nblocks(), init, [](T a, T b) { return b < a ? b : a; });
 }
 
 // ---------------------------------------------------------------------------
@@ -238,11 +243,13 @@ __device__ T team_scan(const Team &t, Scratch &sc, char *sm, int64_t n, In in, O
     if (threadIdx.x == 0) part[t.block()] = s;
     t.sync();
     T base = T(0), total = T(0);
-    for (int b = 0; b < t.nblocks(); ++b) {
-        T x = uread(&part[b]);
+    for (int b = lane_id(); b < t.nblocks(); b += 32) {
+        T x = __ldcg(part + b);
         if (b < t.block()) base += x;
         total += x;
     }
+    base = warp_sum(base);
+    total = warp_sum(total);
     for (int64_t tile = lo; tile < hi; tile += blockDim.x) {
         int64_t i = tile + threadIdx.x;
         T v = i < hi ? in(i) : T(0);
@@ -380,7 +387,11 @@ __device__ __forceinline__ float rsum_warp(int64_t n, Get v)
 // ---------------------------------------------------------------------------
 // LSD radix sort of (uint64 key, V value) pairs, 8-bit digits, stable.
 // The sorted data ends in (*keys, *vals) (pointers may be swapped with the
-// spare buffers).  Two team syncs per pass.
+// spare buffers).  Per pass: each CTA counts the digits of its contiguous
+// chunk into a digit-major table (digit, CTA); an exclusive team scan of that
+// table gives every (digit, CTA) its first output position; each CTA then
+// scatters its chunk tile by tile, ranking keys stably within a warp by
+// match_any.  Four team syncs per pass.
 // ---------------------------------------------------------------------------
 constexpr int SORT_ITEMS = 4;
 
@@ -393,11 +404,11 @@ __device__ void team_sort_pairs(const Team &t, Scratch &sc, char *sm, uint64_t *
     const int NW = blockDim.x >> 5;
     uint64_t am = sc.arena.mark();
     uint32_t *ghist = sc.arena.take<uint32_t>((uint64_t)nb * 256);
+    int64_t *gpos = sc.arena.take<int64_t>((uint64_t)nb * 256);
     if (!sc.arena.ok()) return;
     uint32_t *wcnt = reinterpret_cast<uint32_t *>(sm);              // NW * 256
     int64_t *pos = reinterpret_cast<int64_t *>(sm + NW * 256 * 4);  // 256
     uint32_t *tcnt = reinterpret_cast<uint32_t *>(sm + NW * 256 * 4 + 256 * 8);
-    int64_t *dsm = reinterpret_cast<int64_t *>(sm + NW * 256 * 4 + 256 * 8 + 256 * 4);  // 34
     int64_t lo, hi;
     block_chunk(t, n, lo, hi);
     const int w = warp_in_block();
@@ -407,21 +418,13 @@ __device__ void team_sort_pairs(const Team &t, Scratch &sc, char *sm, uint64_t *
         __syncthreads();
         for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) atomicAdd(&tcnt[(keys[i] >> shift) & 255], 1u);
         __syncthreads();
-        for (int d = threadIdx.x; d < 256; d += blockDim.x) ghist[(int64_t)t.block() * 256 + d] = tcnt[d];
+        for (int d = threadIdx.x; d < 256; d += blockDim.x) ghist[(int64_t)d * nb + t.block()] = tcnt[d];
         t.sync();
-        // 2. global offsets of this CTA's digits
-        int64_t tot = 0, pre = 0;
-        const int d0 = threadIdx.x;
-        if (d0 < 256) {
-            for (int b = 0; b < nb; ++b) {
-                int64_t h = uread(&ghist[(int64_t)b * 256 + d0]);
-                tot += h;
-                if (b < t.block()) pre += h;
-            }
-        }
-        int64_t dummy;
-        int64_t dbase = block_excl_scan<int64_t>(d0 < 256 ? tot : 0, dsm, dummy);
-        if (d0 < 256) pos[d0] = dbase + pre;
+        // 2. first output position of every (digit, CTA)
+        team_scan<Team, int64_t>(
+            t, sc, sm, (int64_t)nb * 256, [&](int64_t i) -> int64_t { return __ldcg(ghist + i); },
+            [&](int64_t i, int64_t pre, int64_t) { gpos[i] = pre; });
+        for (int d = threadIdx.x; d < 256; d += blockDim.x) pos[d] = __ldcg(gpos + (int64_t)d * nb + t.block());
         __syncthreads();
         // 3. stable scatter, one tile of blockDim*SORT_ITEMS keys at a time
         const int64_t TILE = (int64_t)blockDim.x * SORT_ITEMS;
