@@ -146,8 +146,8 @@ int rama_batch_wait(rama_handle h, int64_t *num_labels, double *lbs, int32_t *st
  * RAMA_STATIC_MAX_NODES; larger instances are rejected with
  * RAMA_ERR_INVALID_ARG, and an instance whose solve needs more scratch than
  * the array returns RAMA_ERR_OOM.  dump_timeline is ignored.
- * The first call on a device looks up the array's device address; make that
- * first call before any stream capture.  All calls share the one array: calls
+ * The first call on a device looks up the array's device address and sets the
+ * kernel's shared-memory limit; make that first call before any stream capture.  All calls share the one array: calls
  * that overlap on the GPU (other streams or host threads) race and must be
  * serialised by the caller.
  */

@@ -26,7 +26,6 @@ namespace {
 
 constexpr int THREADS = 512;
 constexpr int SMEM = sort_smem_bytes(THREADS) + 1024;
-constexpr uint64_t PART_BYTES = 16 * 4096;  // >= 16 * (max CTAs + 2)
 constexpr int64_t BLOCK_TEAM_MAX_EDGES = 200000;
 
 thread_local std::string g_err;
@@ -43,23 +42,7 @@ int fail(int code, const std::string &msg)
         if (e_ != cudaSuccess) return fail(RAMA_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
     } while (0)
 
-__device__ __forceinline__ Scratch make_scratch(char *base, uint64_t bytes)
-{
-    Scratch sc;
-    sc.part[0] = base;
-    sc.part[1] = base + PART_BYTES;
-    sc.parity = 0;
-    sc.alg_bytes = 0.0;
-    sc.prof = nullptr;
-    sc.tlast = 0;
-    sc.arena.base = base;
-    sc.arena.cap = bytes - 256;
-    sc.arena.lo = 2 * PART_BYTES;
-    sc.arena.top = sc.arena.cap;
-    sc.arena.peak = sc.arena.lo;
-    sc.arena.failed = 0;
-    return sc;
-}
+__device__ __forceinline__ Scratch make_scratch(char *base, uint64_t bytes) { return scratch_over(base, bytes); }
 
 struct CtaLaunch {
     Instance *inst;
@@ -123,6 +106,8 @@ __device__ void copy_graph_out(const Team &t, const Graph &g, rama_step_args *a)
 template <class Team>
 __device__ void run_step(const Team &t, char *sm, Scratch sc, rama_step_args *a)
 {
+    if (t.rank() == 0) *sc.err = 0;
+    t.sync();
     Graph A;
     A.row = const_cast<int32_t *>(a->row);
     A.col = const_cast<int32_t *>(a->col);
@@ -260,6 +245,7 @@ __device__ void run_step(const Team &t, char *sm, Scratch sc, rama_step_args *a)
     t.sync();
     if (t.leader()) {
         if (!sc.arena.ok()) a->status |= ERR_ARENA;
+        if (__ldcg(sc.err)) a->status |= ERR_ITER_LIMIT;
     }
 }
 
@@ -574,6 +560,10 @@ int rama_create(int device, uint64_t workspace_bytes, rama_handle *out)
     cudaDeviceProp p;
     CU(cudaGetDeviceProperties(&p, device));
     h->sms = p.multiProcessorCount;
+    // the sort stages a tile in shared memory: more than the default 48 KB
+    for (const void *k : {(const void *)k_solve_grid, (const void *)k_solve_cta, (const void *)k_step_grid,
+                          (const void *)k_step_cta, (const void *)k_objective})
+        CU(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
     int per_sm = 0;
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve_grid, THREADS, SMEM));
     if (per_sm < 1) {

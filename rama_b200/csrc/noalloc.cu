@@ -34,7 +34,6 @@ constexpr int THREADS = 512;
 constexpr int SMEM = sort_smem_bytes(THREADS) + 1024;
 constexpr uint64_t STATIC_BYTES = 32ull << 20;
 constexpr uint64_t HEADER_BYTES = 4096;  // the instance descriptor (inputs, options, results)
-constexpr uint64_t PART_BYTES = 16 * 4096;
 static_assert(sizeof(Instance) <= HEADER_BYTES, "instance descriptor does not fit its header");
 
 // The scratch array.  Host code must not hand this name to a kernel: on the
@@ -48,19 +47,7 @@ __global__ void __launch_bounds__(THREADS, 2) k_solve_static(char *scratch)
     BlockTeam t;
     Instance *io = reinterpret_cast<Instance *>(scratch);
     char *base = scratch + HEADER_BYTES;
-    Scratch sc;
-    sc.part[0] = base;
-    sc.part[1] = base + PART_BYTES;
-    sc.parity = 0;
-    sc.alg_bytes = 0.0;
-    sc.prof = nullptr;
-    sc.tlast = 0;
-    sc.arena.base = base;
-    sc.arena.cap = STATIC_BYTES - HEADER_BYTES - 256;
-    sc.arena.lo = 2 * PART_BYTES;
-    sc.arena.top = sc.arena.cap;
-    sc.arena.peak = sc.arena.lo;
-    sc.arena.failed = 0;
+    Scratch sc = scratch_over(base, STATIC_BYTES - HEADER_BYTES);
     // node ids must stay below the limit that the fixed size assumes
     const int32_t *I = io->i, *J = io->j;
     const int32_t mx = team_max<BlockTeam, int32_t>(t, sc, sm, io->n, -1,
@@ -79,7 +66,8 @@ std::mutex g_mutex;
 char *g_address[256] = {};
 
 // Device address of the scratch array on `device`, looked up once per device
-// with that device current.
+// with that device current; the same first call raises the kernel's shared
+// memory limit.
 int scratch_address(int device, char **out)
 {
     std::lock_guard<std::mutex> lock(g_mutex);
@@ -89,6 +77,11 @@ int scratch_address(int device, char **out)
         cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
         if (e != cudaSuccess) {
             rama_set_last_error(std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+            return RAMA_ERR_CUDA;
+        }
+        e = cudaFuncSetAttribute((const void *)k_solve_static, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
+        if (e != cudaSuccess) {
+            rama_set_last_error(std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
             return RAMA_ERR_CUDA;
         }
         g_address[device] = static_cast<char *>(p);

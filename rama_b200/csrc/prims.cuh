@@ -7,6 +7,7 @@
 // index only.
 #pragma once
 #include <cstdint>
+#include <type_traits>
 
 #include "team.cuh"
 
@@ -23,6 +24,7 @@ constexpr unsigned FULL = 0xffffffffu;
 struct Scratch {
     Arena arena;
     char *part[2];  // each >= 16 * (nblocks + 2) bytes
+    int32_t *err;   // set when a bounded wait gave up (zeroed at the start of a solve)
     int parity;
     double alg_bytes;  // algorithmic bytes of the work done (team-uniform tally)
     int64_t *prof;     // optional per-phase nanoseconds (leader only)
@@ -33,6 +35,29 @@ struct Scratch {
         return part[parity];
     }
 };
+
+// A workspace of `bytes` bytes at `base` (256-byte aligned) holds the two
+// partial buffers, the error word and then the arena.
+constexpr uint64_t SCRATCH_PART_BYTES = 16 * 4096;  // >= 16 * (max CTAs + 2)
+
+__device__ __forceinline__ Scratch scratch_over(char *base, uint64_t bytes)
+{
+    Scratch sc;
+    sc.part[0] = base;
+    sc.part[1] = base + SCRATCH_PART_BYTES;
+    sc.err = reinterpret_cast<int32_t *>(base + 2 * SCRATCH_PART_BYTES);
+    sc.parity = 0;
+    sc.alg_bytes = 0.0;
+    sc.prof = nullptr;
+    sc.tlast = 0;
+    sc.arena.base = base;
+    sc.arena.cap = bytes - 256;
+    sc.arena.lo = 2 * SCRATCH_PART_BYTES + 256;
+    sc.arena.top = sc.arena.cap;
+    sc.arena.peak = sc.arena.lo;
+    sc.arena.failed = 0;
+    return sc;
+}
 
 // Phase timing: the team leader charges the time since the last mark to
 // `phase`.  Marks sit right after team syncs, so a phase's time is the span
@@ -385,101 +410,284 @@ __device__ __forceinline__ float rsum_warp(int64_t n, Get v)
 }
 
 // ---------------------------------------------------------------------------
-// LSD radix sort of (uint64 key, V value) pairs, 8-bit digits, stable.
+// LSD radix sort of (uint64 key, 4- or 8-byte value) pairs, 8-bit digits, stable.
 // The sorted data ends in (*keys, *vals) (pointers may be swapped with the
-// spare buffers).  Per pass: each CTA counts the digits of its contiguous
-// chunk into a digit-major table (digit, CTA); an exclusive team scan of that
-// table gives every (digit, CTA) its first output position; each CTA then
-// scatters its chunk tile by tile, ranking keys stably within a warp by
-// match_any.  Four team syncs per pass.
+// spare buffers).
+//
+// One read of the keys counts the digits of every pass at once (a pass only
+// permutes the keys, so its digit totals are known up front).  Each pass then
+// moves the data once.  The input is cut into tiles of blockDim * SORT_ITEMS
+// keys (half as many with 8-byte values); CTA b takes tiles b, b + nblocks,
+// ... in increasing order.  Per tile it
+//   - ranks the keys stably: per-warp digit counters, and ballots over the
+//     digit bits for the lanes holding the same digit;
+//   - finds the tile's output offset per digit by decoupled look-back over
+//     the counts the preceding tiles published;
+//   - stages the tile in digit order in shared memory and writes each digit's
+//     run contiguously.
+// One team sync per pass.  The look-back waits are bounded; a wait that gives
+// up sets the scratch error word and the sort stops with the last complete
+// pass (a permutation of the input).  A single-CTA team keeps running
+// offsets instead of looking back.  A pass in which one digit holds every key
+// is the identity and is skipped.
 // ---------------------------------------------------------------------------
-constexpr int SORT_ITEMS = 4;
+constexpr int SORT_ITEMS = 8;
+constexpr uint64_t LB_VALUE = (uint64_t(1) << 58) - 1;
+constexpr uint64_t LB_AGG = uint64_t(1) << 62;     // tile count published
+constexpr uint64_t LB_PREFIX = uint64_t(2) << 62;  // inclusive prefix published
+constexpr int LB_SPIN_LIMIT = 1 << 20;
+
+__device__ __forceinline__ uint64_t ld_relaxed(const uint64_t *p)
+{
+    uint64_t v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_relaxed(uint64_t *p, uint64_t v)
+{
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// values travel through shared memory as raw 4- or 8-byte words
+template <class V>
+struct SortWord {
+    static_assert(sizeof(V) == 4 || sizeof(V) == 8, "sort values are 4 or 8 bytes");
+    using type = typename std::conditional<sizeof(V) == 8, uint64_t, uint32_t>::type;
+    static __device__ __forceinline__ type to(V v)
+    {
+        type u;
+        memcpy(&u, &v, sizeof(V));
+        return u;
+    }
+    static __device__ __forceinline__ V from(type u)
+    {
+        V v;
+        memcpy(&v, &u, sizeof(V));
+        return v;
+    }
+};
+
+// Decoupled look-back of one tile for all 256 digits: the exclusive count of
+// digit d over tiles [0, tile) in the words of pass tag `tag`.  The CTA loads
+// the published words of LB_WINDOW preceding tiles per digit at once (into
+// `win`, LB_WINDOW * 256 words of shared memory); each digit's thread then
+// adds tile counts from the nearest tile back until it meets an inclusive
+// prefix, or a tile that has not published yet (the next window starts
+// there).  Called by every thread of the CTA; returns the count on threads
+// d < 256.  Waits are bounded: after LB_SPIN_LIMIT rounds without progress
+// the error word is set and the count is left incomplete.
+constexpr int LB_WINDOW = 16;
+
+// bytes of the sort's staging area: a tile of keys and values, or the
+// look-back window, whichever is larger
+__host__ __device__ constexpr int sort_stage_bytes(int threads)
+{
+    return threads * SORT_ITEMS * 12 > LB_WINDOW * 256 * 8 ? threads * SORT_ITEMS * 12 : LB_WINDOW * 256 * 8;
+}
+
+__device__ __forceinline__ int64_t sort_lookback(const uint64_t *flags, int64_t tile, uint64_t tag, uint64_t *win,
+                                                 int64_t *posS, int32_t *err)
+{
+    const int d = threadIdx.x;
+    int64_t excl = 0;
+    bool done = tile == 0;
+    if (d < 256) posS[d] = done ? -1 : tile - 1;
+    int idle = 0;
+    for (;;) {
+        if (!__syncthreads_or(d < 256 && !done)) break;
+        for (int x = threadIdx.x; x < LB_WINDOW * 256; x += blockDim.x) {
+            const int64_t j = posS[x & 255] - (x >> 8);
+            if (posS[x & 255] >= 0) win[x] = j >= 0 ? ld_relaxed(flags + j * 256 + (x & 255)) : (LB_PREFIX | tag);
+        }
+        __syncthreads();
+        bool stuck = false;
+        if (d < 256 && !done) {
+            int64_t pos = posS[d];
+            int k = 0;
+            for (; k < LB_WINDOW; ++k) {
+                const uint64_t w = win[k * 256 + d];
+                if ((w & (uint64_t(15) << 58)) != tag || !(w >> 62)) break;  // not published yet
+                excl += (int64_t)(w & LB_VALUE);
+                if ((w >> 62) == 2) {
+                    done = true;
+                    break;
+                }
+            }
+            stuck = k == 0 && !done;
+            pos -= k;
+            if (done) pos = -1;
+            posS[d] = pos;
+        }
+        if (__syncthreads_or(stuck)) {
+            if (++idle > LB_SPIN_LIMIT || (idle % 1024 == 0 && *(volatile int32_t *)err)) {
+                if (d == 0) atomicOr(err, 1);
+                break;
+            }
+            if (idle > 16) __nanosleep(256);
+        } else {
+            idle = 0;
+        }
+    }
+    return excl;
+}
+
+// Lanes of the warp holding the same 9-bit label (a digit, or 256 for "no
+// key"), from nine ballots over the label's bits.
+__device__ __forceinline__ unsigned warp_peers9(unsigned label)
+{
+    unsigned m = FULL;
+#pragma unroll
+    for (int b = 0; b < 9; ++b) {
+        const unsigned bit = (label >> b) & 1u;
+        const unsigned ball = __ballot_sync(FULL, bit);
+        m &= bit ? ball : ~ball;
+    }
+    return m;
+}
 
 template <class Team, class V>
 __device__ void team_sort_pairs(const Team &t, Scratch &sc, char *sm, uint64_t *&keys, V *&vals, uint64_t *&keys2,
                                 V *&vals2, int64_t n, int bits)
 {
     if (n <= 1 || bits <= 0) return;
+    using W = typename SortWord<V>::type;
+    constexpr int ITEMS = sizeof(V) == 8 ? SORT_ITEMS / 2 : SORT_ITEMS;
+    const int P = (bits + 7) / 8;
     const int nb = t.nblocks();
     const int NW = blockDim.x >> 5;
+    const int TILE = blockDim.x * ITEMS;
+    const int64_t ntiles = (n + TILE - 1) / TILE;
     uint64_t am = sc.arena.mark();
-    uint32_t *ghist = sc.arena.take<uint32_t>((uint64_t)nb * 256);
-    int64_t *gpos = sc.arena.take<int64_t>((uint64_t)nb * 256);
+    uint32_t *ghist = sc.arena.take<uint32_t>(8 * 256);
+    uint64_t *flags = nb > 1 ? sc.arena.take<uint64_t>((uint64_t)ntiles * 256) : nullptr;
     if (!sc.arena.ok()) return;
-    uint32_t *wcnt = reinterpret_cast<uint32_t *>(sm);              // NW * 256
-    int64_t *pos = reinterpret_cast<int64_t *>(sm + NW * 256 * 4);  // 256
-    uint32_t *tcnt = reinterpret_cast<uint32_t *>(sm + NW * 256 * 4 + 256 * 8);
-    int64_t lo, hi;
-    block_chunk(t, n, lo, hi);
+    uint32_t *wcnt = reinterpret_cast<uint32_t *>(sm);  // NW * 256
+    uint64_t *skeys = reinterpret_cast<uint64_t *>(sm + NW * 1024);
+    W *svals = reinterpret_cast<W *>(sm + NW * 1024 + TILE * 8);
+    char *q = sm + NW * 1024 + sort_stage_bytes(blockDim.x);  // staging area: either tile or the window
+    uint32_t *tstart = reinterpret_cast<uint32_t *>(q);
+    int64_t *gbase = reinterpret_cast<int64_t *>(q + 1024);
+    int64_t *bucket = reinterpret_cast<int64_t *>(q + 3072);
+    int64_t *run = reinterpret_cast<int64_t *>(q + 5120);
+    int64_t *ssm = reinterpret_cast<int64_t *>(q + 7168);   // 34
+    int64_t *posS = reinterpret_cast<int64_t *>(q + 7440);  // 256
+    uint64_t *win = skeys;                                  // LB_WINDOW * 256, look-back only
+    uint32_t *lh = reinterpret_cast<uint32_t *>(skeys);    // P * 256, counting only
     const int w = warp_in_block();
-    for (int shift = 0; shift < bits; shift += 8) {
-        // 1. per-CTA digit histogram
-        for (int d = threadIdx.x; d < 256; d += blockDim.x) tcnt[d] = 0;
-        __syncthreads();
-        for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) atomicAdd(&tcnt[(keys[i] >> shift) & 255], 1u);
-        __syncthreads();
-        for (int d = threadIdx.x; d < 256; d += blockDim.x) ghist[(int64_t)d * nb + t.block()] = tcnt[d];
-        t.sync();
-        // 2. first output position of every (digit, CTA)
-        team_scan<Team, int64_t>(
-            t, sc, sm, (int64_t)nb * 256, [&](int64_t i) -> int64_t { return __ldcg(ghist + i); },
-            [&](int64_t i, int64_t pre, int64_t) { gpos[i] = pre; });
-        for (int d = threadIdx.x; d < 256; d += blockDim.x) pos[d] = __ldcg(gpos + (int64_t)d * nb + t.block());
-        __syncthreads();
-        // 3. stable scatter, one tile of blockDim*SORT_ITEMS keys at a time
-        const int64_t TILE = (int64_t)blockDim.x * SORT_ITEMS;
-        for (int64_t tile = lo; tile < hi; tile += TILE) {
+
+    // 0. digit totals of every pass
+    for (int i = threadIdx.x; i < P * 256; i += blockDim.x) lh[i] = 0;
+    for (int64_t i = t.rank(); i < 8 * 256; i += t.size()) ghist[i] = 0;
+    if (flags)
+        for (int64_t i = t.rank(); i < ntiles * 256; i += t.size()) flags[i] = 0;
+    __syncthreads();
+    for (int64_t i = t.rank(); i < n; i += t.size()) {
+        const uint64_t k = keys[i];
+        for (int p = 0; p < P; ++p) atomicAdd(&lh[p * 256 + (int)((k >> (8 * p)) & 255)], 1u);
+    }
+    __syncthreads();
+    t.sync();
+    for (int i = threadIdx.x; i < P * 256; i += blockDim.x)
+        if (lh[i]) atomicAdd(&ghist[i], lh[i]);
+    t.sync();
+
+    for (int p = 0; p < P; ++p) {
+        const int shift = 8 * p;
+        const uint64_t tag = (uint64_t)(p + 1) << 58;
+        const int64_t tot = threadIdx.x < 256 ? (int64_t)__ldcg(ghist + p * 256 + threadIdx.x) : 0;
+        int64_t all;
+        const int64_t ex = block_excl_scan<int64_t>(tot, ssm, all);
+        if (threadIdx.x < 256) {
+            bucket[threadIdx.x] = ex;
+            run[threadIdx.x] = 0;
+        }
+        if (__syncthreads_or(threadIdx.x < 256 && tot == n)) continue;  // identity pass
+        for (int64_t tile = t.block(); tile < ntiles; tile += nb) {
+            const int64_t t0 = tile * TILE;
+            const int tn = (int)((n - t0) < TILE ? (n - t0) : TILE);
             for (int d = lane_id(); d < 256; d += 32) wcnt[w * 256 + d] = 0;
-            __syncwarp();
-            const int64_t sub = tile + (int64_t)w * 32 * SORT_ITEMS;
-            uint64_t mk[SORT_ITEMS];
-            V mv[SORT_ITEMS];
-            int md[SORT_ITEMS];
-            uint32_t mr[SORT_ITEMS];
+            uint64_t mk[ITEMS];
+            W mv[ITEMS];
+            uint32_t mr[ITEMS];
+            const int wb = w * 32 * ITEMS;
 #pragma unroll
-            for (int k = 0; k < SORT_ITEMS; ++k) {
-                int64_t idx = sub + k * 32 + lane_id();
-                bool valid = idx < hi;
-                uint64_t key = valid ? keys[idx] : 0;
-                int d = valid ? int((key >> shift) & 255) : 256;
-                unsigned peers = __match_any_sync(FULL, d);
-                int leader = __ffs(peers) - 1;
+            for (int k = 0; k < ITEMS; ++k) {
+                const int li = wb + k * 32 + lane_id();
+                const bool valid = li < tn;
+                mk[k] = valid ? keys[t0 + li] : 0;
+                mv[k] = valid ? SortWord<V>::to(vals[t0 + li]) : W(0);
+            }
+            __syncwarp();
+            // 1. stable rank within the warp
+#pragma unroll
+            for (int k = 0; k < ITEMS; ++k) {
+                const bool valid = wb + k * 32 + lane_id() < tn;
+                const int d = valid ? (int)((mk[k] >> shift) & 255) : 256;
+                const unsigned peers = warp_peers9((unsigned)d);
+                const int leader = __ffs(peers) - 1;
                 uint32_t b0 = 0;
                 if (valid && lane_id() == leader) {
                     b0 = wcnt[w * 256 + d];
                     wcnt[w * 256 + d] = b0 + __popc(peers);
                 }
                 b0 = __shfl_sync(FULL, b0, leader);
-                __syncwarp();
-                mk[k] = key;
-                mv[k] = valid ? vals[idx] : V();
-                md[k] = d;
                 mr[k] = b0 + __popc(peers & lanemask_lt());
+                __syncwarp();
             }
             __syncthreads();
-            for (int d = threadIdx.x; d < 256; d += blockDim.x) {
-                uint32_t s = 0;
-                for (int q = 0; q < NW; ++q) {
-                    uint32_t c = wcnt[q * 256 + d];
-                    wcnt[q * 256 + d] = s;
-                    s += c;
+            // 2. per digit: offsets of the warps, the tile's count and start
+            uint32_t cnt = 0;
+            if (threadIdx.x < 256) {
+                for (int qw = 0; qw < NW; ++qw) {
+                    const uint32_t c = wcnt[qw * 256 + threadIdx.x];
+                    wcnt[qw * 256 + threadIdx.x] = cnt;
+                    cnt += c;
                 }
-                tcnt[d] = s;
             }
+            int64_t tt;
+            const int64_t ts = block_excl_scan<int64_t>((int64_t)cnt, ssm, tt);
+            // 3. output offset of the tile per digit
+            if (threadIdx.x < 256) tstart[threadIdx.x] = (uint32_t)ts;
+            int64_t excl = 0;
+            if (nb == 1) {
+                if (threadIdx.x < 256) {
+                    excl = run[threadIdx.x];
+                    run[threadIdx.x] = excl + cnt;
+                }
+            } else {
+                if (threadIdx.x < 256)
+                    st_relaxed(flags + tile * 256 + threadIdx.x, (tile == 0 ? LB_PREFIX : LB_AGG) | tag | (uint64_t)cnt);
+                excl = sort_lookback(flags, tile, tag, win, posS, sc.err);
+                if (threadIdx.x < 256 && tile > 0)
+                    st_relaxed(flags + tile * 256 + threadIdx.x, LB_PREFIX | tag | (uint64_t)(excl + cnt));
+            }
+            if (threadIdx.x < 256) gbase[threadIdx.x] = bucket[threadIdx.x] + excl;
             __syncthreads();
+            // 4. stage the tile in digit order
 #pragma unroll
-            for (int k = 0; k < SORT_ITEMS; ++k) {
-                if (md[k] < 256) {
-                    int64_t p = pos[md[k]] + wcnt[w * 256 + md[k]] + mr[k];
-                    keys2[p] = mk[k];
-                    vals2[p] = mv[k];
+            for (int k = 0; k < ITEMS; ++k) {
+                if (wb + k * 32 + lane_id() < tn) {
+                    const int d = (int)((mk[k] >> shift) & 255);
+                    const uint32_t loc = tstart[d] + wcnt[w * 256 + d] + mr[k];
+                    skeys[loc] = mk[k];
+                    svals[loc] = mv[k];
                 }
             }
             __syncthreads();
-            for (int d = threadIdx.x; d < 256; d += blockDim.x) pos[d] += tcnt[d];
+            // 5. write the digit runs
+            for (int i = threadIdx.x; i < tn; i += blockDim.x) {
+                const uint64_t key = skeys[i];
+                const int d = (int)((key >> shift) & 255);
+                const int64_t dst = gbase[d] + (i - (int64_t)tstart[d]);
+                if (dst >= 0 && dst < n) {
+                    keys2[dst] = key;
+                    vals2[dst] = SortWord<V>::from(svals[i]);
+                }
+            }
             __syncthreads();
         }
         t.sync();
+        if (__ldcg(sc.err)) break;  // keep the last complete pass
         uint64_t *tk = keys;
         keys = keys2;
         keys2 = tk;
@@ -493,7 +701,7 @@ __device__ void team_sort_pairs(const Team &t, Scratch &sc, char *sm, uint64_t *
 // shared-memory bytes the sort needs for a CTA of `threads` threads
 __host__ __device__ constexpr int sort_smem_bytes(int threads)
 {
-    return (threads / 32) * 256 * 4 + 256 * 8 + 256 * 4 + 34 * 8;
+    return (threads / 32) * 1024 + sort_stage_bytes(threads) + 7440 + 256 * 8;
 }
 
 // ---------------------------------------------------------------------------

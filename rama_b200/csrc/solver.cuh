@@ -63,6 +63,7 @@ template <class Team>
 __device__ void solve_instance(const Team &t, char *sm, Scratch sc, Instance *io)
 {
     const Options o = io->opts;
+    if (t.rank() == 0) *sc.err = 0;  // the first team primitive below syncs before any reader
     sc.prof = io->prof;
     if (sc.prof && t.leader()) sc.tlast = prof_now();
     const int64_t n = io->n;
@@ -197,6 +198,7 @@ __device__ void solve_instance(const Team &t, char *sm, Scratch sc, Instance *io
         }
     }
     t.sync();
+    if (__ldcg(sc.err)) status |= ERR_ITER_LIMIT;
     if (t.leader()) {
         io->status = status;
         io->lb = lb;

@@ -168,12 +168,25 @@ def test_csum(solver, oracle, n, team):
 
 
 @pytest.mark.parametrize("team", TEAMS)
-@pytest.mark.parametrize("n,bits", [(1, 8), (1000, 5), (100_000, 20), (300_001, 44)])
+@pytest.mark.parametrize("n,bits", [(1, 8), (1000, 5), (100_000, 20), (300_001, 44), (1_000_000, 3),
+                                    (3_000_017, 44)])
 def test_radix_sort_is_stable(solver, n, bits, team):
     rng = np.random.default_rng(bits)
     keys = rng.integers(0, 1 << bits, size=n, dtype=np.uint64)
     vals = np.arange(n, dtype=np.int32)
     gk, gv = solver.step_sort(keys, vals, bits, team=team)
+    order = np.argsort(keys, kind="stable")
+    assert np.array_equal(gk, keys[order])
+    assert np.array_equal(gv, vals[order])
+
+
+@pytest.mark.parametrize("team", TEAMS)
+def test_radix_sort_skips_constant_digits(solver, team):
+    """Digits that are equal in every key leave the order as it is."""
+    rng = np.random.default_rng(5)
+    keys = (rng.integers(0, 256, size=200_000, dtype=np.uint64) << np.uint64(16)) | np.uint64(7)
+    vals = np.arange(len(keys), dtype=np.int32)
+    gk, gv = solver.step_sort(keys, vals, 32, team=team)
     order = np.argsort(keys, kind="stable")
     assert np.array_equal(gk, keys[order])
     assert np.array_equal(gv, vals[order])
