@@ -10,7 +10,7 @@ events on the launch stream; `e2e` runs the same solve through the C ABI's
 host entry point (rama_solve_host: host arrays in, labels out).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--config c1|c2|c2p|c3|c4]
+                    [--config c1|c2|c2p|c3|c4|c5] [--requests R] [--rates 100,1000,5000]
 
 --impl reference times the reference solver built from source for sm_100a
 (oracle/_ref/librama_ref.so, its rama_cuda entry points) on the same
@@ -42,6 +42,8 @@ CONFIGS = {
     "c3": dict(desc="random geometric k-NN graph, 1M points, k=20, D (dual only)", mode="D"),
     "c4": dict(desc="512 Delaunay region-adjacency graphs, n log-uniform [500,20000], batched PD", mode="PD"),
     "c2s": dict(desc="3-D grid 64x64x32 + long range (profiling-size C2), PD", mode="PD"),
+    "c5": dict(desc="served: Poisson arrivals of grids 16^3..128^3, Delaunay 1e3..2e6 edges, k-NN (k=10) "
+                    "1e4..5e5 nodes; modes P/PD/D 50/40/10%", mode="mixed"),
 }
 
 
@@ -176,6 +178,8 @@ def run_ours(args, rank, world, local):
     mode = CONFIGS[cfg]["mode"]
     if cfg == "c4":
         return run_ours_batch(args, rank, world, local)
+    if cfg == "c5":
+        return run_ours_served(args, rank, world, local)
     i, j, c = make_instance(cfg)
     E = len(c)
     dev = torch.device("cuda", local)
@@ -349,6 +353,93 @@ def run_ours_batch(args, rank, world, local):
     }
 
 
+def run_ours_served(args, rank, world, local):
+    """Continuous batching of a Poisson request stream (rama_b200.server).
+
+    A pool of distinct request graphs (seeded, the served mix's kinds and size
+    ranges, pinned in host memory) stands in for the clients; each request of
+    the stream is a pool graph with its own mode.  Per arrival rate the server
+    serves `--requests` requests in real time: every request's graph is copied
+    host -> device when its lane admits it and its labels come back to the
+    host, so the numbers are end to end.  `value` = edges/s at the highest
+    rate; `plain` = the same requests solved one at a time (each alone on its
+    automatic team) on a bounded sample.  Ranks serve separate streams."""
+    import torch
+
+    from rama_b200 import instances as I
+    from rama_b200 import server as S
+    from rama_b200.solver import Solver
+
+    rates = [float(x) for x in args.rates.split(",")]
+    t_gen = time.perf_counter()
+    pool = I.served_pool(size=args.pool, seed=1005 + rank)
+    pinned = [tuple(torch.from_numpy(np.ascontiguousarray(x)).pin_memory() for x in g) for g in pool]
+    nodes = [int(max(g[0].max(), g[1].max())) + 1 for g in pool]
+    gen_s = time.perf_counter() - t_gen
+    srv = S.Server(device=local, lanes=args.lanes, lane_bytes=args.lane_gb << 30, max_batch=256)
+    # warm-up: every pool graph once, all queued at once
+    warm = [S.Request(k, *pinned[k], mode="PD", num_nodes=nodes[k]) for k in range(len(pool))]
+    for _ in range(max(1, args.warmup // 3)):
+        srv.serve(warm, realtime=False)
+    per_rate = []
+    lanes_alg0 = sum(ln.alg_bytes for ln in srv.lanes)
+    with Clocks(local) as clk:
+        for rate in rates:
+            stream = I.served_stream(num_requests=args.requests, rate=rate, pool_size=len(pool), seed=1006 + rank)
+            reqs = [S.Request(k, *pinned[p], mode=m, arrival=t, num_nodes=nodes[p]) for k, (t, m, p) in
+                    enumerate(stream)]
+            barrier(world)
+            st = srv.serve(reqs, realtime=True)
+            bad = sum(r.status != 0 for r in reqs)
+            summ = st.summary()
+            summ.update(rate_per_s=rate, failed=bad, h2d_bytes=int(sum(12 * r.num_edges for r in reqs)),
+                        d2h_bytes=int(sum(4 * r.num_nodes for r in reqs)))
+            per_rate.append(summ)
+    alg = sum(ln.alg_bytes for ln in srv.lanes) - lanes_alg0
+    busy_s = sum(x["wall_s"] for x in per_rate)
+    srv.close()
+    # plain form: the first requests of the last stream, one solve at a time
+    s = Solver(local)
+    sample = reqs[: min(len(reqs), args.plain_sample)]
+    plain_ms, plain_edges = 0.0, 0
+    for r in sample:
+        d = [x.to(torch.device("cuda", local), non_blocking=True) for x in (r.i, r.j, r.c)]
+        s.solve_device(*d, mode=r.mode)
+        torch.cuda.synchronize()
+        plain_ms += s.stats().device_ms
+        plain_edges += r.num_edges
+    if rank != 0:
+        return None
+    top = per_rate[-1]
+    hbm, src = peaks()
+    achieved = alg / busy_s / 1e9 if busy_s else 0.0
+    value = world * top["edges_per_s"]
+    return {
+        "metric": "edges/s", "value": value, "unit": "edges/s", "n_gpus": world, "steps": len(rates),
+        "warmup": args.warmup, "ms_per_step": top["wall_s"] * 1e3, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32 (costs, messages) / f64 (bound, objective)",
+        "data": "synthetic (seeded pool of request graphs with the served mix's kinds and size ranges)",
+        "config": {"workload": CONFIGS["c5"]["desc"], "requests_per_rate": args.requests, "rates_per_s": rates,
+                   "pool_graphs": len(pool), "pool_edges": int(sum(len(g[2]) for g in pool)),
+                   "lanes": args.lanes, "lane_bytes": args.lane_gb << 30,
+                   "parallelism": "continuous batching: lanes = handle + stream + fixed HBM budget; instances "
+                                  "on 8-CTA clusters or one CTA each"},
+        "solves_per_s": world * top["solves_per_s"],
+        "served": per_rate,
+        "plain": {"value": plain_edges / (plain_ms / 1e3) if plain_ms else 0.0, "unit": "edges/s",
+                  "solves_per_s": len(sample) / (plain_ms / 1e3) if plain_ms else 0.0, "requests": len(sample),
+                  "device_ms": plain_ms, "form": "one request per launch, device time only"},
+        "e2e": {"value": value, "unit": "edges/s", "h2d_bytes_per_step": top["h2d_bytes"],
+                "d2h_bytes_per_step": top["d2h_bytes"], "api": "rama_b200.server.Server.serve"},
+        "gpu_launches": int(sum(x["batches"] for x in per_rate)),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
+                     "traffic": None, "peak_source": src, "kernel": "k_solve_mixed / k_solve_cta",
+                     "algorithmic_bytes": alg, "note": "algorithmic bytes of all served batches / served wall time"},
+        "pool_generation_s": gen_s,
+        "clocks": clk.summary(),
+    }
+
+
 def cpu_baseline(cfg, mode):
     from oracle import oracle_py as O
 
@@ -376,6 +467,63 @@ def cpu_baseline(cfg, mode):
             "host_cores": os.cpu_count()}
 
 
+def run_reference_many(args, local, R):
+    """Reference arm of the batched (c4) and served (c5) configs: the reference
+    has no batch or serving API, so its form is one rama_cuda call per
+    instance; a bounded sample of the same instances is timed with CUDA
+    events around each call."""
+    import torch
+
+    from rama_b200 import instances as I
+
+    cfg = args.config
+    if cfg == "c4":
+        batch = I.delaunay_batch(seed=1004)
+        insts = [(batch.instance(k), "PD") for k in range(batch.count)]
+        sample = insts[: args.ref_sample]
+        what = "the first %d of the 512 Delaunay graphs, PD, one rama_cuda call each" % len(sample)
+    else:
+        pool = I.served_pool(size=args.pool, seed=1005)
+        stream = I.served_stream(num_requests=args.requests, rate=1000.0, pool_size=len(pool), seed=1006)
+        sample = [(pool[p], m) for (_, m, p) in stream[: args.ref_sample]]
+        what = "the first %d requests of the served stream, one rama_cuda call each" % len(sample)
+    dev = torch.device("cuda", local)
+    stream_ = torch.cuda.current_stream(dev)
+    times, edges = [], 0
+    with Clocks(local) as clk:
+        for w, ((i, j, c), mode) in enumerate(sample[: args.warmup] + sample):
+            E = len(c)
+            N = int(max(i.max(), j.max())) + 1
+            d_i, d_j, d_c = (torch.from_numpy(np.ascontiguousarray(x)).to(dev) for x in (i, j, c))
+            lab = torch.empty(N, dtype=torch.int32, device=dev)
+            ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            ev0.record(stream_)
+            R.rama_device(C.c_void_p(d_i.data_ptr()), C.c_void_p(d_j.data_ptr()), C.c_void_p(d_c.data_ptr()), E,
+                          C.c_void_p(lab.data_ptr()), N, mode)
+            ev1.record(stream_)
+            torch.cuda.synchronize()
+            if w >= args.warmup:
+                times.append(ev0.elapsed_time(ev1))
+                edges += E
+    tot_s = sum(times) / 1e3
+    value = edges / tot_s
+    lat = np.asarray(times)
+    return {
+        "impl": "reference", "metric": "edges/s", "value": value, "unit": "edges/s", "n_gpus": 1,
+        "steps": len(times), "warmup": args.warmup, "ms_per_step": float(lat.mean()), "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": CONFIGS[cfg]["desc"], "sample": what, "edges": edges},
+        "solves_per_s": len(times) / tot_s, "p50_ms": float(np.percentile(lat, 50)),
+        "p99_ms": float(np.percentile(lat, 99)),
+        "e2e": {"value": value, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "cpu_baseline": {"value": value, "unit": "edges/s", "cores": 0, "kind": "reference",
+                         "sample": what + " (the reference solver built from source for sm_100a; it has no CPU "
+                                          "path)"},
+        "clocks": clk.summary(),
+    }
+
+
 def run_reference(args, rank, world, local):
     if rank != 0:
         return None
@@ -386,6 +534,8 @@ def run_reference(args, rank, world, local):
     import torch
 
     torch.cuda.set_device(local)
+    if args.config in ("c4", "c5"):
+        return run_reference_many(args, local, R)
     cfg = args.config
     mode = CONFIGS[cfg]["mode"]
     i, j, c = make_instance(cfg)
@@ -448,8 +598,18 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--team", type=int, default=0, help="0 auto, 1 one CTA, 2 cooperative grid")
+    ap.add_argument("--team", type=int, default=0, help="0 auto, 1 one CTA, 2 cooperative grid, 3 cluster")
+    ap.add_argument("--requests", type=int, default=2000, help="c5: requests per arrival rate")
+    ap.add_argument("--rates", default="100,1000,5000", help="c5: arrival rates per second")
+    ap.add_argument("--pool", type=int, default=32, help="c5: distinct request graphs")
+    ap.add_argument("--lanes", type=int, default=12, help="c5: server lanes")
+    ap.add_argument("--lane-gb", type=int, default=8, help="c5: HBM budget per lane (GiB)")
+    ap.add_argument("--plain-sample", type=int, default=200, help="c5: requests solved one at a time")
+    ap.add_argument("--ref-sample", type=int, default=64, help="c4/c5 reference arm: instances timed")
     args = ap.parse_args()
+    if args.config == "c5":
+        # lanes overlap only when each stream has its own hardware queue
+        os.environ.setdefault("CUDA_DEVICE_MAX_CONNECTIONS", str(max(8, args.lanes)))
     rank, world, local = dist_setup(args.gpus)
     if args.impl == "reference":
         line = run_reference(args, rank, world, local)

@@ -44,7 +44,12 @@ typedef struct {
     int32_t dump_timeline;
     int32_t verbose;
     int32_t sanitize_graph;
-    int32_t team; /* 0 = choose by size, 1 = one CTA, 2 = whole GPU (cooperative grid) */
+    /* execution team: 1 = one CTA, 2 = whole GPU (cooperative grid), 3 = one cluster of 8
+     * CTAs, 0 = choose by size (one CTA below 4,000 edges, a cluster below 100,000, else the
+     * whole GPU).  In a batch, 1 keeps an instance on one CTA, 2 and 3 put it on a cluster,
+     * and 0 puts it on a cluster when it has at least 20,000 edges and more than 1.5 times
+     * the batch's edges per CTA. */
+    int32_t team;
 } rama_options;
 
 /* Presets of multicut_solver_options(const std::string&) (reference
@@ -56,7 +61,11 @@ typedef struct rama_context *rama_handle;
 
 /* A handle owns the device workspace (reused across calls) and its streams.
  * workspace_bytes = 0 picks a size from the first problem and grows it when
- * needed.  Not thread-safe: use one handle per host thread. */
+ * needed.  workspace_bytes > 0 fixes the workspace: it is allocated whole at
+ * the first call and never grows; a batch whose instance slices (1024 bytes
+ * per edge + 1 MiB per instance, rounded up to 4 KiB) add up to more is
+ * refused with RAMA_ERR_OOM.  Not thread-safe: use one handle per host
+ * thread. */
 int rama_create(int device, uint64_t workspace_bytes, rama_handle *out);
 void rama_destroy(rama_handle h);
 
@@ -67,7 +76,7 @@ typedef struct {
     int32_t mst_rounds;
     int32_t timeline_rounds;
     int32_t dual_oom;        /* the dual ran out of workspace and fell back to the trivial bound */
-    int32_t team;            /* 1 = CTA, 2 = grid */
+    int32_t team;            /* 1 = CTA, 2 = grid, 3 = cluster */
     int64_t triangles;       /* triangle counter of the initial dual's last pass */
     int64_t edges_after_dual;
     int64_t workspace_peak;  /* bytes */

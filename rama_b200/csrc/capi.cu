@@ -26,7 +26,10 @@ namespace {
 
 constexpr int THREADS = 512;
 constexpr int SMEM = sort_smem_bytes(THREADS) + 1024;
-constexpr int64_t BLOCK_TEAM_MAX_EDGES = 200000;
+constexpr int CLUSTER_CTAS = 8;               // CTAs of a cluster team (the portable maximum)
+constexpr int64_t CLUSTER_MIN_EDGES = 20000;   // smaller batch instances always run on one CTA
+constexpr int64_t SINGLE_CLUSTER_MIN = 4000;   // a single solve from this size on runs on a cluster
+constexpr int64_t GRID_MIN_EDGES = 100000;     // ... and from this size on on the whole GPU
 
 thread_local std::string g_err;
 
@@ -65,6 +68,56 @@ __global__ void __launch_bounds__(THREADS, 2) k_solve_cta(CtaLaunch L)
         Instance *io = &L.inst[L.order[k]];
         Scratch sc = make_scratch(io->ws, io->ws_bytes);
         solve_instance(t, sm, sc, io);
+        __syncthreads();
+    }
+}
+
+// A batch with instances for clusters: clusters of CLUSTER_CTAS CTAs draw
+// from the queue, which holds the cluster instances first (largest first);
+// once a cluster draws an instance that is not for a cluster, its CTAs go on
+// alone, one instance each, like k_solve_cta.
+struct MixedLaunch {
+    Instance *inst;
+    const int32_t *order;
+    int32_t count;
+    int32_t ncluster;  // queue entries [0, ncluster) are solved by a cluster
+    int32_t *queue;
+};
+
+__global__ void __launch_bounds__(THREADS, 2) k_solve_mixed(MixedLaunch L)
+{
+    extern __shared__ __align__(16) char sm[];
+    __shared__ int next;
+    cg::cluster_group cl = cg::this_cluster();
+    ClusterTeam ct;
+    BlockTeam bt;
+    int mine = -1;  // an instance this CTA drew for itself
+    for (int guard = 0; guard < (1 << 30); ++guard) {
+        if (cl.block_rank() == 0 && threadIdx.x == 0) next = atomicAdd(L.queue, 1);
+        cl.sync();
+        const int k = *cl.map_shared_rank(&next, 0);
+        cl.sync();  // no CTA reads another's shared memory after this point
+        if (k >= L.count) return;
+        if (k >= L.ncluster) {
+            if (cl.block_rank() == 0) mine = k;
+            break;
+        }
+        Instance *io = &L.inst[L.order[k]];
+        solve_instance(ct, sm, make_scratch(io->ws, io->ws_bytes), io);
+        cl.sync();
+    }
+    for (int guard = 0; guard < (1 << 30); ++guard) {
+        int k = mine;
+        mine = -1;
+        if (k < 0) {
+            if (threadIdx.x == 0) next = atomicAdd(L.queue, 1);
+            __syncthreads();
+            k = next;
+            __syncthreads();
+        }
+        if (k >= L.count) break;
+        Instance *io = &L.inst[L.order[k]];
+        solve_instance(bt, sm, make_scratch(io->ws, io->ws_bytes), io);
         __syncthreads();
     }
 }
@@ -315,6 +368,7 @@ struct rama_context {
     int step_ctas = 0;  // ... of k_step_grid
     int obj_ctas = 0;   // ... of k_objective
     int cta_per_sm = 0;
+    int cluster_max = 0;  // co-resident clusters of k_solve_mixed
     char *ws = nullptr;
     uint64_t ws_bytes = 0;
     uint64_t ws_fixed = 0;  // user-requested size (0 = automatic)
@@ -343,6 +397,7 @@ struct rama_context {
     Instance *b_host = nullptr;  // pinned: instance descriptors in, results out
     int32_t b_host_cap = 0;
     std::vector<Instance> b_in;
+    std::vector<char> b_cluster;  // instance k is solved by a cluster team
     std::vector<int32_t> b_order;
     cudaEvent_t ev_done = nullptr;
 };
@@ -389,13 +444,34 @@ uint64_t ws_estimate(int64_t n_edges) { return (uint64_t)n_edges * 1024ull + (64
 // workspace slice of one instance of a batch
 uint64_t ws_slice(int64_t n_edges) { return ((uint64_t)n_edges * 1024ull + (1ull << 20) + 4095) & ~uint64_t(4095); }
 
-// Launches the solve of the instances already in h->d_inst.  team 1: CTAs.
-int launch_solve(rama_context *h, int32_t count, int team, cudaStream_t st)
+// Launches the solve of the instances already in h->d_inst (queue order in
+// h->d_order).  team 2: one instance on the cooperative grid; otherwise the
+// first `ncluster` queue entries go to cluster teams and the rest to CTAs.
+int launch_solve(rama_context *h, int32_t count, int team, cudaStream_t st, int32_t ncluster = 0)
 {
     if (team == 2) {
         GridLaunch L{h->d_inst, h->ws, h->ws_bytes};
         void *args[] = {&L};
         CU(cudaLaunchCooperativeKernel((void *)k_solve_grid, dim3(h->grid_ctas), dim3(THREADS), args, SMEM, st));
+    } else if (ncluster > 0) {
+        const int64_t want = (int64_t)ncluster * CLUSTER_CTAS + (count - ncluster);
+        const int64_t cap = (int64_t)std::max(1, h->cluster_max) * CLUSTER_CTAS;
+        const int64_t ctas = (std::min(want, cap) + CLUSTER_CTAS - 1) / CLUSTER_CTAS * CLUSTER_CTAS;
+        CU(cudaMemsetAsync(h->d_queue, 0, sizeof(int32_t), st));
+        MixedLaunch L{h->d_inst, h->d_order, count, ncluster, h->d_queue};
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)ctas);
+        cfg.blockDim = dim3(THREADS);
+        cfg.dynamicSmemBytes = SMEM;
+        cfg.stream = st;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = CLUSTER_CTAS;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        CU(cudaLaunchKernelEx(&cfg, k_solve_mixed, L));
     } else {
         const int ctas = std::max(1, std::min<int>(count, h->sms * h->cta_per_sm));
         CU(cudaMemsetAsync(h->d_queue, 0, sizeof(int32_t), st));
@@ -413,7 +489,7 @@ int solve_one(rama_context *h, const int32_t *d_i, const int32_t *d_j, const flo
     if (!h || !opts || n < 0 || (n > 0 && (!d_i || !d_j || !d_c))) return fail(RAMA_ERR_INVALID_ARG, "bad arguments");
     Options o = to_opts(opts);
     int team = opts->team;
-    if (team != 1 && team != 2) team = (n <= BLOCK_TEAM_MAX_EDGES) ? 1 : 2;
+    if (team < 1 || team > 3) team = n < SINGLE_CLUSTER_MIN ? 1 : (n < GRID_MIN_EDGES ? 3 : 2);
     int rc = ensure_inst(h, 1);
     if (rc) return rc;
     // timeline buffer
@@ -450,7 +526,7 @@ int solve_one(rama_context *h, const int32_t *d_i, const int32_t *d_j, const flo
         CU(cudaMemcpyAsync(h->d_inst, &hi, sizeof(Instance), cudaMemcpyHostToDevice, st));
         CU(cudaMemcpyAsync(h->d_order, &zero, sizeof(int32_t), cudaMemcpyHostToDevice, st));
         CU(cudaEventRecord(h->ev0, st));
-        rc = launch_solve(h, 1, team, st);
+        rc = launch_solve(h, 1, team, st, team == 3 ? 1 : 0);
         if (rc) return rc;
         CU(cudaEventRecord(h->ev1, st));
         Instance ho{};
@@ -561,8 +637,8 @@ int rama_create(int device, uint64_t workspace_bytes, rama_handle *out)
     CU(cudaGetDeviceProperties(&p, device));
     h->sms = p.multiProcessorCount;
     // the sort stages a tile in shared memory: more than the default 48 KB
-    for (const void *k : {(const void *)k_solve_grid, (const void *)k_solve_cta, (const void *)k_step_grid,
-                          (const void *)k_step_cta, (const void *)k_objective})
+    for (const void *k : {(const void *)k_solve_grid, (const void *)k_solve_cta, (const void *)k_solve_mixed,
+                          (const void *)k_step_grid, (const void *)k_step_cta, (const void *)k_objective})
         CU(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
     int per_sm = 0;
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve_grid, THREADS, SMEM));
@@ -578,6 +654,22 @@ int rama_create(int device, uint64_t workspace_bytes, rama_handle *out)
     int per_sm_cta = 0;
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_cta, k_solve_cta, THREADS, SMEM));
     h->cta_per_sm = std::max(1, per_sm_cta);
+    {
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(CLUSTER_CTAS);
+        cfg.blockDim = dim3(THREADS);
+        cfg.dynamicSmemBytes = SMEM;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = CLUSTER_CTAS;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int ncl = 0;
+        CU(cudaOccupancyMaxActiveClusters(&ncl, (void *)k_solve_mixed, &cfg));
+        h->cluster_max = std::max(1, ncl);
+    }
     CU(cudaMalloc(&h->d_queue, sizeof(int32_t) * 4));
     CU(cudaMalloc(&h->d_step, sizeof(rama_step_args)));
     CU(cudaMalloc(&h->d_scalar, sizeof(double) * 4));
@@ -707,6 +799,7 @@ int rama_batch_launch(rama_handle h, const int32_t *d_i, const int32_t *d_j, con
         h->b_host_cap = count;
     }
     h->b_in.assign(count, Instance{});
+    h->b_cluster.assign(count, 0);
     h->b_order.resize(count);
     for (int32_t k = 0; k < count; ++k) {
         const int64_t a = edge_offsets[k], b = edge_offsets[k + 1];
@@ -720,13 +813,35 @@ int rama_batch_launch(rama_handle h, const int32_t *d_i, const int32_t *d_j, con
         x.labels_cap = label_offsets[k + 1] - label_offsets[k];
         h->b_order[k] = k;
     }
-    std::stable_sort(h->b_order.begin(), h->b_order.end(),
-                     [&](int32_t x, int32_t y) { return h->b_in[x].n > h->b_in[y].n; });
+    // Automatic teams: an instance goes to a cluster when one CTA alone would
+    // take much longer than the batch as a whole, i.e. when it holds more than
+    // 1.5 times the edges per CTA of the batch (a cluster finishes it sooner
+    // but spends more CTA time on it).
+    {
+        int64_t total_edges = 0;
+        for (int32_t k = 0; k < count; ++k) total_edges += h->b_in[k].n;
+        const int64_t per_cta = total_edges / std::max(1, h->sms * h->cta_per_sm);
+        const int64_t auto_min = std::max<int64_t>(CLUSTER_MIN_EDGES, per_cta + per_cta / 2);
+        for (int32_t k = 0; k < count; ++k) {
+            const int tm = opts[opts_count == 1 ? 0 : k].team;
+            h->b_cluster[k] = (tm == 2 || tm == 3 || ((tm < 1 || tm > 3) && h->b_in[k].n >= auto_min)) ? 1 : 0;
+        }
+    }
+    // queue order: cluster instances first, then by size, largest first
+    std::stable_sort(h->b_order.begin(), h->b_order.end(), [&](int32_t x, int32_t y) {
+        if (h->b_cluster[x] != h->b_cluster[y]) return h->b_cluster[x] > h->b_cluster[y];
+        return h->b_in[x].n > h->b_in[y].n;
+    });
+    int32_t ncluster = 0;
+    for (int32_t k = 0; k < count; ++k) ncluster += h->b_cluster[k];
     // every instance owns a workspace slice sized from its edge count; their
     // sum is the batch's device footprint
     uint64_t total = 0;
     for (int32_t k = 0; k < count; ++k) total += ws_slice(h->b_in[k].n);
-    rc = ensure_ws(h, total);
+    // a handle with a fixed workspace allocates all of it once and admits
+    // batches up to that size
+    if (h->ws_fixed && total > h->ws_fixed) return fail(RAMA_ERR_OOM, "batch exceeds the handle's fixed workspace");
+    rc = ensure_ws(h, h->ws_fixed ? h->ws_fixed : total);
     if (rc) return rc;
     if (h->ws_bytes < total) return fail(RAMA_ERR_OOM, "workspace too small for the batch");
     {
@@ -741,7 +856,7 @@ int rama_batch_launch(rama_handle h, const int32_t *d_i, const int32_t *d_j, con
     CU(cudaMemcpyAsync(h->d_inst, h->b_host, sizeof(Instance) * count, cudaMemcpyHostToDevice, st));
     CU(cudaMemcpyAsync(h->d_order, h->b_order.data(), sizeof(int32_t) * count, cudaMemcpyHostToDevice, st));
     CU(cudaEventRecord(h->ev0, st));
-    rc = launch_solve(h, count, 1, st);
+    rc = launch_solve(h, count, 1, st, ncluster);
     if (rc) return rc;
     CU(cudaEventRecord(h->ev1, st));
     CU(cudaMemcpyAsync(h->b_host, h->d_inst, sizeof(Instance) * count, cudaMemcpyDeviceToHost, st));
@@ -779,10 +894,15 @@ int rama_batch_wait(rama_handle h, int64_t *num_labels, double *lbs, int32_t *st
         if (redo.empty()) break;
         uint64_t total = 0;
         for (int32_t k : redo) total += h->b_in[k].ws_bytes * 2;
+        if (h->ws_fixed && total > h->ws_fixed) break;  // they stay out of workspace
         int rc = ensure_ws(h, total);
         if (rc) return rc;
         std::vector<int32_t> order(redo.size());
         std::iota(order.begin(), order.end(), 0);
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int32_t x, int32_t y) { return h->b_cluster[redo[x]] > h->b_cluster[redo[y]]; });
+        int32_t ncl = 0;
+        for (int32_t k : redo) ncl += h->b_cluster[k];
         std::vector<Instance> sub(redo.size());
         uint64_t off = 0;
         for (size_t q = 0; q < redo.size(); ++q) {
@@ -796,7 +916,7 @@ int rama_batch_wait(rama_handle h, int64_t *num_labels, double *lbs, int32_t *st
         CU(cudaMemcpyAsync(h->d_inst, sub.data(), sizeof(Instance) * sub.size(), cudaMemcpyHostToDevice, h->b_stream));
         CU(cudaMemcpyAsync(h->d_order, order.data(), sizeof(int32_t) * order.size(), cudaMemcpyHostToDevice,
                            h->b_stream));
-        rc = launch_solve(h, (int32_t)sub.size(), 1, h->b_stream);
+        rc = launch_solve(h, (int32_t)sub.size(), 1, h->b_stream, ncl);
         if (rc) return rc;
         CU(cudaMemcpyAsync(sub.data(), h->d_inst, sizeof(Instance) * sub.size(), cudaMemcpyDeviceToHost, h->b_stream));
         CU(cudaStreamSynchronize(h->b_stream));

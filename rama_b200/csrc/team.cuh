@@ -5,9 +5,13 @@
 //               in a batch); sync() is __syncthreads().
 //   GridTeam  : every thread of a cooperative grid (one large instance);
 //               sync() is a grid-wide barrier.
+//   ClusterTeam: the CTAs of one thread-block cluster (mid-size instances,
+//               several at once); sync() is the hardware cluster barrier.
+//               The hardware schedules a cluster's CTAs together, so its
+//               members may wait on one another like a grid's.
 // Work decomposition inside a phase uses only rank()/size() (grid-stride) or
 // block()/nblocks() (one contiguous chunk per CTA, for order-preserving scans,
-// compactions and sorts), so the same code is correct for both teams and its
+// compactions and sorts), so the same code is correct for every team and its
 // results do not depend on the team size.
 #pragma once
 #include <cooperative_groups.h>
@@ -23,6 +27,15 @@ struct BlockTeam {
     __device__ __forceinline__ int nblocks() const { return 1; }
     __device__ __forceinline__ void sync() const { __syncthreads(); }
     __device__ __forceinline__ bool leader() const { return threadIdx.x == 0; }
+};
+
+struct ClusterTeam {
+    __device__ __forceinline__ int rank() const { return (int)cg::this_cluster().block_rank() * blockDim.x + threadIdx.x; }
+    __device__ __forceinline__ int size() const { return (int)cg::this_cluster().num_blocks() * blockDim.x; }
+    __device__ __forceinline__ int block() const { return (int)cg::this_cluster().block_rank(); }
+    __device__ __forceinline__ int nblocks() const { return (int)cg::this_cluster().num_blocks(); }
+    __device__ __forceinline__ void sync() const { cg::this_cluster().sync(); }
+    __device__ __forceinline__ bool leader() const { return cg::this_cluster().block_rank() == 0 && threadIdx.x == 0; }
 };
 
 struct GridTeam {

@@ -8,7 +8,8 @@ and cost distributions as the benchmark configurations:
 * ``grid3d_longrange`` 256x256x64 voxel grid, 6-neighbour + long-range offsets
 * ``knn_rgg``          random geometric k-NN graph (k=20 on 1M points)
 * ``delaunay``         Delaunay adjacency of random points (region adjacency graphs)
-* ``served_mix``       a Poisson arrival stream mixing the above
+* ``served_pool`` / ``served_stream``  request graphs mixing the above and a
+  Poisson arrival stream over them
 
 Every instance is (i, j, costs) with int32 node ids, i != j, each undirected
 edge once, and float32 costs; positive cost = attractive.
@@ -157,33 +158,38 @@ def random_graph(n, avg_deg, seed, neg_frac=0.4, scale=1.0):
     return i, j, c
 
 
-def served_mix(num_requests=10000, rate=1000.0, seed=1005, max_edges=None):
-    """Poisson arrivals mixing grids, Delaunay graphs and k-NN graphs.
+def served_instance(rng, max_edges=None):
+    """One request graph of the served mix: a grid cube (side 16..128,
+    6-neighbour), a Delaunay graph (1e3..2e6 edges, log-uniform) or a k-NN
+    graph (k = 10, 1e4..5e5 nodes, log-uniform), each kind with probability
+    1/3; costs N(0.2, 1) with 5% of the edges at -5.  `max_edges` bounds the
+    size (quick tests) by drawing smaller parameters, not by cutting edges."""
+    kind = int(rng.integers(0, 3))
+    lim = float("inf") if max_edges is None else float(max_edges)
+    if kind == 0:
+        hi = int(min(128, max(16, (lim / 3) ** (1 / 3))))
+        return _cube(int(rng.integers(16, hi + 1)), rng)
+    if kind == 1:
+        ne = math.exp(rng.uniform(math.log(1e3), math.log(min(2e6, max(lim, 1e3)))))
+        return delaunay(max(int(ne / 3), 16), rng)
+    nn = int(math.exp(rng.uniform(math.log(1e4), math.log(min(5e5, max(lim / 7, 1e4))))))
+    return _knn_small(nn, 10, rng)
 
-    Returns a list of (arrival_time_s, mode, (i, j, c)).  Grid sides 16..128
-    (cubes, 6-neighbour), Delaunay 1e3..2e6 edges log-uniform, k-NN k=10 with
-    1e4..5e5 nodes; modes P/PD/D at 50/40/10%.  `max_edges` caps instance size
-    (used by quick tests).
-    """
+
+def served_pool(size=48, seed=1005, max_edges=None):
+    """`size` distinct request graphs of the served mix (see served_instance)."""
+    rng = np.random.default_rng(seed)
+    return [served_instance(rng, max_edges) for _ in range(size)]
+
+
+def served_stream(num_requests=10000, rate=1000.0, pool_size=48, seed=1006):
+    """A Poisson arrival stream over a pool of request graphs: a list of
+    (arrival time in seconds, mode, pool index).  Modes P/PD/D at 50/40/10%."""
     rng = np.random.default_rng(seed)
     t = np.cumsum(rng.exponential(1.0 / rate, size=num_requests))
-    out = []
-    for k in range(num_requests):
-        kind = rng.integers(0, 3)
-        mode = rng.choice(["P", "PD", "D"], p=[0.5, 0.4, 0.1])
-        if kind == 0:
-            side = int(rng.integers(16, 129))
-            inst = _cube(side, rng)
-        elif kind == 1:
-            ne = math.exp(rng.uniform(math.log(1e3), math.log(2e6)))
-            inst = delaunay(max(int(ne / 3), 16), rng)
-        else:
-            nn = int(math.exp(rng.uniform(math.log(1e4), math.log(5e5))))
-            inst = _knn_small(nn, 10, rng)
-        if max_edges is not None and len(inst[2]) > max_edges:
-            inst = tuple(x[:max_edges] for x in inst)
-        out.append((float(t[k]), str(mode), inst))
-    return out
+    modes = rng.choice(["P", "PD", "D"], size=num_requests, p=[0.5, 0.4, 0.1])
+    idx = rng.integers(0, pool_size, size=num_requests)
+    return [(float(t[k]), str(modes[k]), int(idx[k])) for k in range(num_requests)]
 
 
 def _cube(side, rng):

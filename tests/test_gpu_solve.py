@@ -22,7 +22,7 @@ CASES = cases()
 IDS = [c[0] for c in CASES]
 
 
-@pytest.mark.parametrize("team", (1, 2))
+@pytest.mark.parametrize("team", (1, 2, 3))
 @pytest.mark.parametrize("mode", ("P", "PD", "PD+", "D"))
 @pytest.mark.parametrize("case", CASES, ids=IDS)
 def test_solve_matches_oracle(solver, oracle, case, mode, team):
@@ -61,6 +61,22 @@ def test_invalid_input_is_rejected(solver):
 def test_empty_instance(solver):
     lab, lb, _ = solver.solve(np.zeros(0, np.int32), np.zeros(0, np.int32), np.zeros(0, np.float32))
     assert len(lab) == 0 and lb == 0.0
+
+
+def test_batch_with_clusters_equals_single_solves(solver, oracle):
+    """Instances of 20,000 edges and more go to cluster teams, the rest to
+    CTAs; every result equals the oracle's."""
+    rng = np.random.default_rng(8)
+    insts = [instances.delaunay(int(n), rng) for n in (9000, 300, 12000, 7000, 50, 2500)]
+    insts += [instances.random_graph(5000, 6, seed=12), instances.grid2d(150, 150, seed=6)]
+    batch = instances.pack(insts)
+    for mode in ("PD", "D"):
+        res, status, rc = solver.solve_batch(batch, mode=mode)
+        assert rc == 0 and not status.any()
+        for k, (i, j, c) in enumerate(insts):
+            olab, olb, _ = oracle.solve(i, j, c, mode)
+            assert np.array_equal(res[k][0], olab)
+            assert res[k][1] == olb
 
 
 def test_batch_equals_single_solves(solver, oracle):
