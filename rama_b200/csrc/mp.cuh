@@ -3,9 +3,12 @@
 //
 // Layout (all SoA in the arena): triangles t1<t2<t3 sorted and unique; their
 // edge indices e12/e13/e23 into the merged edge list (the graph's edges plus
-// the triangle chords it lacks, cost 0); per-edge incidence lists (3t+slot,
-// in triangle order) that replace the reference's float atomicAdd by a
-// deterministic RSUM per edge.
+// the triangle chords it lacks, cost 0).  The messages a triangle sends to
+// its edges go to `slot`, which holds each edge's incoming messages
+// contiguously in incidence order (triangle order); pos[3t + corner] is the
+// slot of triangle t's message to that corner's edge.  Each edge then takes
+// the RSUM of its run of slots, which replaces the reference's float
+// atomicAdd by a deterministic sum.
 #pragma once
 #include "cycles.cuh"
 
@@ -16,13 +19,13 @@ struct Mp {
     int32_t *t1, *t2, *t3;
     int32_t *e12, *e13, *e23;
     float *c12, *c13, *c23;
-    float *diff;  // 3T
+    float *slot;  // 3T: incoming messages, edge by edge in incidence order
+    int32_t *pos;  // 3T: slot of triangle t's message to corner c at 3t + c
     int32_t *row, *col;
     float *cost;
     float *share;      // E: cost / number of incident triangles (covered edges)
-    int32_t *inc_off;  // E + 1
-    int32_t *inc;      // 3T
-    int32_t *longe;    // edges with more than 32 incident triangles
+    int32_t *inc_off;  // E + 1: first slot of each edge
+    int32_t *longe;    // edges with more than RSUM_THREAD_MAX incident triangles
     int64_t nlong;
     int32_t rows, cols;
 };
@@ -137,12 +140,12 @@ __device__ bool mp_build(const Team &t, Scratch &sc, char *sm, const Graph &A, T
     mp.c12 = sc.arena.take<float>(T + 1);
     mp.c13 = sc.arena.take<float>(T + 1);
     mp.c23 = sc.arena.take<float>(T + 1);
-    mp.diff = sc.arena.take<float>(3 * T + 1);
-    mp.inc = sc.arena.take<int32_t>(3 * T + 1);
+    mp.slot = sc.arena.take<float>(3 * T + 1);
+    mp.pos = sc.arena.take<int32_t>(3 * T + 1);
     mp.inc_off = sc.arena.take<int32_t>(E + 2);
     uint64_t ik = sc.arena.mark();
     uint64_t *q1 = sc.arena.take<uint64_t>(3 * T + 1), *q2 = sc.arena.take<uint64_t>(3 * T + 1);
-    int32_t *w2 = sc.arena.take<int32_t>(3 * T + 1);
+    int32_t *w1 = sc.arena.take<int32_t>(3 * T + 1), *w2 = sc.arena.take<int32_t>(3 * T + 1);
     if (!sc.arena.ok()) return false;
     for (int64_t k = t.rank(); k < T; k += t.size()) {
         int32_t a = mp.t1[k], b = mp.t2[k], c = mp.t3[k];
@@ -156,18 +159,17 @@ __device__ bool mp_build(const Team &t, Scratch &sc, char *sm, const Graph &A, T
         q1[3 * k] = (uint64_t)x;
         q1[3 * k + 1] = (uint64_t)y;
         q1[3 * k + 2] = (uint64_t)z;
-        mp.inc[3 * k] = (int32_t)(3 * k);
-        mp.inc[3 * k + 1] = (int32_t)(3 * k + 1);
-        mp.inc[3 * k + 2] = (int32_t)(3 * k + 2);
+        w1[3 * k] = (int32_t)(3 * k);
+        w1[3 * k + 1] = (int32_t)(3 * k + 1);
+        w1[3 * k + 2] = (int32_t)(3 * k + 2);
     }
     t.sync();
-    // incidence lists: stable sort of (edge, 3t+slot) by edge
-    int32_t *incp = mp.inc;
+    // incidence order: stable sort of (edge, 3t + corner) by edge; the rank of
+    // each (triangle, corner) in that order is its slot
+    int32_t *incp = w1;
     uint64_t *qk = q1;
     team_sort_pairs(t, sc, sm, qk, incp, q2, w2, 3 * T, bits_for((uint64_t)(E > 0 ? E : 1)));
-    if (incp != mp.inc) {
-        for (int64_t k = t.rank(); k < 3 * T; k += t.size()) mp.inc[k] = incp[k];
-    }
+    for (int64_t q = t.rank(); q < 3 * T; q += t.size()) mp.pos[incp[q]] = (int32_t)q;
     team_offsets(t, 3 * T, (int32_t)E, [&](int64_t k) { return (int32_t)qk[k]; }, mp.inc_off);
     sc.arena.release(ik);
     // each covered edge's share of its cost, and the edges whose incoming
@@ -176,7 +178,7 @@ __device__ bool mp_build(const Team &t, Scratch &sc, char *sm, const Graph &A, T
     mp.longe = sc.arena.take<int32_t>(E + 1);
     if (!sc.arena.ok()) return false;
     mp.nlong = team_compact(
-        t, sc, sm, E, [&](int64_t e) { return mp.inc_off[e + 1] - mp.inc_off[e] > 32; },
+        t, sc, sm, E, [&](int64_t e) { return mp.inc_off[e + 1] - mp.inc_off[e] > RSUM_THREAD_MAX; },
         [&](int64_t e, int64_t p) { mp.longe[p] = (int32_t)e; });
     for (int64_t e = t.rank(); e < E; e += t.size()) {
         const int32_t n = mp.inc_off[e + 1] - mp.inc_off[e];
@@ -274,23 +276,23 @@ __device__ void mp_iteration(const Team &t, const Mp &mp)
         mp.c12[k] = t12;
         mp.c13[k] = t13;
         mp.c23[k] = t23;
-        mp.diff[3 * k] = e12;
-        mp.diff[3 * k + 1] = e13;
-        mp.diff[3 * k + 2] = e23;
+        mp.slot[mp.pos[3 * k]] = e12;
+        mp.slot[mp.pos[3 * k + 1]] = e13;
+        mp.slot[mp.pos[3 * k + 2]] = e23;
     }
     t.sync();
-    // covered edges: c = 0 + RSUM(messages); long lists by a warp
+    // covered edges: c = 0 + RSUM(messages); long runs by a warp
     for (int64_t e = t.rank(); e < mp.E; e += t.size()) {
         const int32_t s = mp.inc_off[e], n = mp.inc_off[e + 1] - s;
-        if (n == 0 || n > 32) continue;
-        const float c = __fadd_rn(0.0f, rsum_serial(n, [&](int k) { return mp.diff[mp.inc[s + k]]; }));
+        if (n == 0 || n > RSUM_THREAD_MAX) continue;
+        const float c = __fadd_rn(0.0f, rsum_upto8(mp.slot + s, n));
         mp.cost[e] = c;
         mp.share[e] = __fdiv_rn(c, (float)n);
     }
     for (int64_t q = team_warp(t); q < mp.nlong; q += team_nwarps(t)) {
         const int32_t e = mp.longe[q];
         const int32_t s = mp.inc_off[e], n = mp.inc_off[e + 1] - s;
-        const float c = __fadd_rn(0.0f, rsum_warp(n, [&](int64_t k) { return mp.diff[mp.inc[s + k]]; }));
+        const float c = __fadd_rn(0.0f, rsum_warp(n, [&](int64_t k) { return mp.slot[s + k]; }));
         if (lane_id() == 0) {
             mp.cost[e] = c;
             mp.share[e] = __fdiv_rn(c, (float)n);

@@ -395,6 +395,22 @@ __device__ __forceinline__ float rsum_serial(int n, Get v)
     return (float)r;
 }
 
+// The same sum by one thread for n <= 8 values at p[0, n): the loads are
+// independent and issued together, then a fixed tree over 8 values padded
+// with +0.0.  Adding an exact zero changes no sum, so this equals
+// rsum_serial(n, p[k]).
+constexpr int RSUM_THREAD_MAX = 8;
+
+__device__ __forceinline__ float rsum_upto8(const float *p, int n)
+{
+    double x[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = k < n ? __dadd_rn(0.0, (double)p[k]) : 0.0;
+    const double a = __dadd_rn(__dadd_rn(x[0], x[1]), __dadd_rn(x[2], x[3]));
+    const double b = __dadd_rn(__dadd_rn(x[4], x[5]), __dadd_rn(x[6], x[7]));
+    return (float)__dadd_rn(a, b);
+}
+
 // the same sum by a whole warp (any n); result valid on every lane
 template <class Get>
 __device__ __forceinline__ float rsum_warp(int64_t n, Get v)
