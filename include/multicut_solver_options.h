@@ -28,6 +28,9 @@ struct multicut_solver_options {
     bool dump_timeline = false;
     bool verbose = true;
     bool sanitize_graph = false;
+    // not in the reference: also cut conflicted 5-cycles in the forest
+    // contraction (its check_pentagons_cuda, shipped disabled there)
+    bool woc_pentagons = false;
 
     multicut_solver_options() {}
     multicut_solver_options(const std::string &solver_type)
@@ -90,6 +93,7 @@ struct multicut_solver_options {
         o.verbose = verbose;
         o.sanitize_graph = sanitize_graph;
         o.team = team;
+        o.woc_pentagons = woc_pentagons;
         return o;
     }
 
@@ -118,6 +122,8 @@ struct multicut_solver_options {
                 dump_timeline = true;
             else if (a == "--sanitize_graph")
                 sanitize_graph = true;
+            else if (a == "--woc_pentagons")
+                woc_pentagons = true;
             else if (a.size() > 1 && a[0] == '-' && !(a[1] >= '0' && a[1] <= '9') && a[1] != '.')
                 return err("The following argument was not expected: " + a);
             else
@@ -181,7 +187,8 @@ struct multicut_solver_options {
                "  -o,--out_sol_file FILE   Path to save node labeling (.txt)\n"
                "  --only_lb                Only compute the lower bound.\n"
                "  --dump_timeline          Return the output of each contraction step.\n"
-               "  --sanitize_graph         Relabel nodes without edges; their label is -1.\n";
+               "  --sanitize_graph         Relabel nodes without edges; their label is -1.\n"
+               "  --woc_pentagons          Also cut conflicted 5-cycles in forest contractions.\n";
     }
     static int range_int(const std::string &s, int lo, int hi, const char *name)
     {

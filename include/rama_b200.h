@@ -50,6 +50,10 @@ typedef struct {
      * and 0 puts it on a cluster when it has at least 20,000 edges and more than 1.5 times
      * the batch's edges per CTA. */
     int32_t team;
+    /* 1: the forest contraction also cuts conflicted 5-cycles of the forest
+     * (check_pentagons_cuda, src/edge_contractions_woc.cu:81-139, which the
+     * reference ships disabled); 0 (default) as the reference. */
+    int32_t woc_pentagons;
 } rama_options;
 
 /* Presets of multicut_solver_options(const std::string&) (reference
@@ -180,7 +184,8 @@ enum {
     RAMA_STEP_INIT = 1,       /* (i,j,c) -> sorted graph            dCOO::init       src/dCOO.cu:28-55 */
     RAMA_STEP_CONTRACT = 2,   /* graph + map -> contracted graph     contract_cuda    src/dCOO.cu:57-95 */
     RAMA_STEP_MATCHING = 3,   /* graph -> map, nr                    rama_cuda.cu:54-62 */
-    RAMA_STEP_WOC = 4,        /* graph -> map, nr                    edge_contractions_woc.cu:387-423 */
+    RAMA_STEP_WOC = 4,        /* graph -> map, nr                    edge_contractions_woc.cu:387-423
+                                 (max_cycle_length >= 5 adds the pentagon check, :81-139) */
     RAMA_STEP_MSF = 5,        /* (i,j,w) -> chosen flags             gpuMST.cu:364-388 */
     RAMA_STEP_CC = 6,         /* CSR -> labels                       ECL-CC_11.cu:315-350 */
     RAMA_STEP_CYCLES = 7,     /* graph -> triangles                  conflicted_cycles_cuda.cu:222-343 */

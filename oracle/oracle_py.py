@@ -35,6 +35,7 @@ class OrcOpts(C.Structure):
         ("dump_timeline", C.c_int32),
         ("verbose", C.c_int32),
         ("sanitize_graph", C.c_int32),
+        ("woc_pentagons", C.c_int32),
     ]
 
 
@@ -92,6 +93,7 @@ def lib():
         L.orc_matching.argtypes = [_G, C.c_float, _i32p, C.POINTER(_i64), C.POINTER(C.c_int32)]
         L.orc_msf.argtypes = [_i64, _i32p, _i32p, _f32p, _i32p, C.POINTER(_i64)]
         L.orc_woc.argtypes = [_G, _i32p, C.POINTER(_i64), C.POINTER(C.c_int32)]
+        L.orc_woc_ex.argtypes = [_G, _i32p, C.POINTER(_i64), C.POINTER(C.c_int32), C.c_int]
         L.orc_conflicted_cycles.argtypes = [_G, C.c_int32, C.c_float, C.c_float, _i32p, _i64, C.POINTER(_i64),
                                             C.POINTER(_i64)]
         L.orc_mp_create.restype = C.c_void_p
@@ -229,12 +231,12 @@ def msf(i, j, w):
     return out[: k.value].copy()
 
 
-def woc(g: Graph):
+def woc(g: Graph, pentagons=False):
     cap = g.max_dim() + 1
     out = np.zeros(cap, np.int32)
     size = _i64(0)
     nr = C.c_int32(0)
-    lib().orc_woc(g.ptr, out, C.byref(size), C.byref(nr))
+    lib().orc_woc_ex(g.ptr, out, C.byref(size), C.byref(nr), int(bool(pentagons)))
     return out[: size.value].copy(), nr.value
 
 

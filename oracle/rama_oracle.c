@@ -801,6 +801,47 @@ static int forest_check_quadrangles(forest_t *F)
     return any;
 }
 
+/* check_pentagons_cuda (src/edge_contractions_woc.cu:81-139, called from the
+ * commented-out line :414): for a repulsive edge (v1, v2), forest neighbours
+ * n1 of v1 and n2 of v2 (n1 != n2) and the first common neighbour mid of n1
+ * and n2, cut the weakest of the four forest edges of v1-n1-mid-n2-v2 in the
+ * reference's comparison order. */
+static int forest_check_pentagons(forest_t *F)
+{
+    if (F->R == 0) return 0;
+    uint8_t *inv = (uint8_t *)xcalloc((size_t)F->m2, 1);
+    for (int64_t k = 0; k < F->R; ++k) {
+        int32_t v1 = F->rr[k], v2 = F->rc[k];
+        for (int32_t e2 = F->off[v2]; e2 < F->off[v2 + 1]; ++e2) {
+            for (int32_t e1 = F->off[v1]; e1 < F->off[v1 + 1]; ++e1) {
+                int32_t n1 = F->c[e1], n2 = F->c[e2];
+                if (n1 == n2) continue;
+                int32_t p1, p2;
+                if (first_common(F->off, F->c, n1, n2, &p1, &p2) < 0) continue;
+                float a = F->w[e1], b = F->w[e2], c1 = F->w[p1], c2 = F->w[p2];
+                if (a < b) {
+                    if (a < c1 && a < c2)
+                        inv[e1] = 1;
+                    else if (c1 < c2)
+                        inv[p1] = 1;
+                    else
+                        inv[p2] = 1;
+                } else {
+                    if (b < c1 && b < c2)
+                        inv[e2] = 1;
+                    else if (c1 < c2)
+                        inv[p1] = 1;
+                    else
+                        inv[p2] = 1;
+                }
+            }
+        }
+    }
+    int any = forest_remove_mask(F, inv);
+    free(inv);
+    return any;
+}
+
 /* filter_by_thresholding (src/edge_contractions_woc_thrust.cu:522-542) */
 static int forest_threshold(forest_t *F)
 {
@@ -977,6 +1018,11 @@ static int forest_resolve(forest_t *F, const rooted_t *T, const int32_t *plen, i
 
 int orc_woc(const orc_graph *A, int32_t *map_out, int64_t *map_size, int32_t *nr_out)
 {
+    return orc_woc_ex(A, map_out, map_size, nr_out, 0);
+}
+
+int orc_woc_ex(const orc_graph *A, int32_t *map_out, int64_t *map_size, int32_t *nr_out, int pentagons)
+{
     forest_t F;
     memset(&F, 0, sizeof(F));
     F.nn = graph_max_dim(A);
@@ -1040,6 +1086,7 @@ int orc_woc(const orc_graph *A, int32_t *map_out, int64_t *map_size, int32_t *nr
         forest_filter_by_cc(&F);
         if (forest_check_triangles(&F)) forest_filter_by_cc(&F);
         forest_check_quadrangles(&F);
+        if (pentagons) forest_check_pentagons(&F);
         if (F.m2 > 0) {
             /* edge_contractions_woc_thrust::find_contraction_mapping (:544-599) */
             int64_t R = forest_filter_by_cc(&F);
@@ -1666,6 +1713,7 @@ void orc_opts_init(orc_opts *o, const char *mode)
     o->dump_timeline = 0;
     o->verbose = 0;
     o->sanitize_graph = 0;
+    o->woc_pentagons = 0;
     if (!mode) return;
     if (strcmp(mode, "P") == 0) {
         o->max_cycle_length_lb = 0;
@@ -1809,7 +1857,7 @@ int orc_solve(int64_t n, const int32_t *i, const int32_t *j, const float *c, con
                 st.matching_rounds++;
                 if ((float)nr < (float)A->rows * o->matching_thresh_crossover_ratio) try_mm = 0;
             } else {
-                orc_woc(A, map, &msize, &nr);
+                orc_woc_ex(A, map, &msize, &nr, o->woc_pentagons);
                 st.mst_rounds++;
             }
             if (nr == 0) break;

@@ -42,6 +42,7 @@ typedef struct {
     int32_t dump_timeline;
     int32_t verbose;
     int32_t sanitize_graph;
+    int32_t woc_pentagons; /* the forest contraction's 5-cycle check, disabled in the reference */
 } orc_opts;
 
 /* Directed COO graph (the reference's dCOO, include/dCOO.h:13-70):
@@ -96,6 +97,8 @@ int orc_msf(int64_t m, const int32_t *i, const int32_t *j, const float *w, int32
 /* conflict-free forest contraction (edge_contractions_woc{,_thrust}.cu); map has
  * max(rows,cols) entries; nr = directed forest entries left (0 = stop). */
 int orc_woc(const orc_graph *A, int32_t *map_out, int64_t *map_size, int32_t *nr_out);
+/* orc_woc with the 5-cycle forest check (check_pentagons_cuda) when pentagons != 0 */
+int orc_woc_ex(const orc_graph *A, int32_t *map_out, int64_t *map_size, int32_t *nr_out, int pentagons);
 
 /* ---- conflicted cycles ---- */
 /* writes the first min(count, budget) emitted triangles (3 ints each) in

@@ -22,7 +22,15 @@
 #include "conflicted_cycles_cuda.h"
 #include "dCOO.h"
 #include "dual_solver.h"
+// The forest contraction's 5-cycle check is a private member that the
+// reference never calls (the call at src/edge_contractions_woc.cu:414 is
+// commented out).  To pin the oracle's optional pentagon step against the
+// reference's own kernel, this test harness opens the class and runs the same
+// sequence as find_contraction_mapping with that call enabled.
+#define private public
 #include "edge_contractions_woc.h"
+#undef private
+#include "edge_contractions_woc_thrust.h"
 #include "gpuMST.h"
 #include "maximum_matching_vertex_based.h"
 #include "multicut_message_passing.h"
@@ -238,6 +246,35 @@ int ref_woc(int64_t E, const int *row, const int *col, const float *cost, int ro
     thrust::copy(m.begin(), m.end(), map_out);
     *map_size = (int64_t)m.size();
     *nr = n;
+    GUARD_END
+}
+
+// edge_contractions_woc::find_contraction_mapping (src/edge_contractions_woc.cu:386-423)
+// with its commented-out check_pentagons() call (:414) enabled
+int ref_woc_pentagons(int64_t E, const int *row, const int *col, const float *cost, int rows, int cols, int *map_out,
+                      int64_t map_cap, int64_t *map_size, int *nr)
+{
+    GUARD_BEGIN
+    dCOO A = make_sorted(E, row, col, cost, rows, cols);
+    edge_contractions_woc w(A, false);
+    *map_size = 0;
+    *nr = 0;
+    if (w.mst_row_ids.size() > 0) {
+        w.filter_by_cc();
+        if (w.check_triangles()) w.filter_by_cc();
+        w.check_quadrangles();
+        w.check_pentagons();
+        edge_contractions_woc_thrust mapper(w.num_nodes, std::move(w.mst_row_ids), std::move(w.mst_col_ids),
+                                            std::move(w.mst_data), std::move(w.rep_row_ids),
+                                            std::move(w.rep_col_ids), std::move(w.cc_labels), false);
+        thrust::device_vector<int> m;
+        int n;
+        std::tie(m, n) = mapper.find_contraction_mapping();
+        if ((int64_t)m.size() > map_cap) throw std::runtime_error("map capacity too small");
+        thrust::copy(m.begin(), m.end(), map_out);
+        *map_size = (int64_t)m.size();
+        *nr = n;
+    }
     GUARD_END
 }
 

@@ -46,6 +46,7 @@ def lib():
         L.ref_dual.argtypes = [_i64, _i32p, _i32p, _f32p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_float, C.c_int,
                                _PD, _P64, _i32p, _i32p, _f32p, _PI, _PI, _i64]
         L.ref_woc.argtypes = [_i64, _i32p, _i32p, _f32p, C.c_int, C.c_int, _i32p, _i64, _P64, _PI]
+        L.ref_woc_pentagons.argtypes = [_i64, _i32p, _i32p, _f32p, C.c_int, C.c_int, _i32p, _i64, _P64, _PI]
         L.ref_rama.argtypes = [_i64, _i32p, _i32p, _f32p, _i32p, _f32p, _i32p, _i64, _P64, _PD, _PI]
         L.ref_rama_device.argtypes = [_i64, C.c_void_p, C.c_void_p, C.c_void_p, _i32p, _f32p, C.c_void_p, _i64,
                                       _P64, _PD]
@@ -147,12 +148,15 @@ def dual(row, col, cost, rows, cols, max_len, num_iter, tri_factor=2.0, num_oute
     return lb.value, r[:k], co[:k], w[:k], ro.value, cc_.value
 
 
-def woc(row, col, cost, rows, cols):
+def woc(row, col, cost, rows, cols, pentagons=False):
+    """The reference's forest contraction; `pentagons` runs it with its
+    (otherwise disabled) 5-cycle forest check."""
     row, col, cost = _a32(row), _a32(col), _f32(cost)
     cap = max(rows, cols) + 2
     out = np.zeros(cap, np.int32)
     sz, nr = _i64(0), C.c_int(0)
-    _check(lib().ref_woc(len(cost), row, col, cost, rows, cols, out, cap, C.byref(sz), C.byref(nr)))
+    f = lib().ref_woc_pentagons if pentagons else lib().ref_woc
+    _check(f(len(cost), row, col, cost, rows, cols, out, cap, C.byref(sz), C.byref(nr)))
     return out[: sz.value], nr.value
 
 

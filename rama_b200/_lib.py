@@ -39,6 +39,7 @@ class RamaOptions(C.Structure):
         ("verbose", C.c_int32),
         ("sanitize_graph", C.c_int32),
         ("team", C.c_int32),
+        ("woc_pentagons", C.c_int32),
     ]
 
 

@@ -186,7 +186,7 @@ __device__ void run_step(const Team &t, char *sm, Scratch sc, rama_step_args *a)
     } else if (op == RAMA_STEP_WOC) {
         int32_t sz = 0;
         int err = 0;
-        int32_t nr = woc_contraction_map(t, sc, sm, A, a->out_map, &sz, &err);
+        int32_t nr = woc_contraction_map(t, sc, sm, A, a->out_map, &sz, &err, a->max_cycle_length >= 5);
         if (t.leader()) {
             a->out_nr = nr;
             a->out_count = sz;
@@ -353,6 +353,7 @@ Options to_opts(const rama_options *o)
     r.dump_timeline = o->dump_timeline;
     r.verbose = o->verbose;
     r.sanitize_graph = o->sanitize_graph;
+    r.woc_pentagons = o->woc_pentagons;
     return r;
 }
 
@@ -605,6 +606,7 @@ int rama_options_init(rama_options *o, const char *mode)
     o->verbose = 0;
     o->sanitize_graph = 0;
     o->team = 0;
+    o->woc_pentagons = 0;
     if (!mode) return RAMA_OK;
     if (!strcmp(mode, "P")) {
         o->max_cycle_length_lb = 0;

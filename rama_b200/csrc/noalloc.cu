@@ -106,6 +106,7 @@ Options options_of(const rama_options *o)
     r.dump_timeline = 0;  // no timeline: it would need memory of its own
     r.verbose = o->verbose;
     r.sanitize_graph = o->sanitize_graph;
+    r.woc_pentagons = o->woc_pentagons;
     return r;
 }
 

@@ -22,6 +22,7 @@ struct Options {
     int32_t dump_timeline;
     int32_t verbose;
     int32_t sanitize_graph;
+    int32_t woc_pentagons;
 };
 
 // One instance: inputs, outputs and statistics (device memory).
@@ -131,7 +132,7 @@ __device__ void solve_instance(const Team &t, char *sm, Scratch sc, Instance *io
                         ++mrounds;
                         if ((float)nr < (float)A.rows * o.matching_thresh_crossover_ratio) try_mm = false;
                     } else {
-                        nr = woc_contraction_map(t, sc, sm, A, map, &msize, &werr);
+                        nr = woc_contraction_map(t, sc, sm, A, map, &msize, &werr, o.woc_pentagons != 0);
                         prof_mark(t, sc, PH_WOC);
                         ++wrounds;
                         status |= werr;

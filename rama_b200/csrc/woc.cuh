@@ -259,6 +259,39 @@ __device__ bool forest_check_quadrangles(const Team &t, Scratch &sc, char *sm, F
     return forest_remove_flagged(t, sc, sm, F);
 }
 
+// check_pentagons_cuda (src/edge_contractions_woc.cu:81-139): for every
+// repulsive edge (v1, v2) and every pair of forest neighbours n1 of v1, n2 of
+// v2 with n1 != n2, the first common neighbour mid of n1 and n2 closes the
+// 5-cycle v1-n1-mid-n2-v2; the weakest of its four forest edges is cut (the
+// reference's comparison order).  The reference ships this step disabled;
+// here it runs when the option asks for it.
+template <class Team>
+__device__ bool forest_check_pentagons(const Team &t, Scratch &sc, char *sm, Forest &F)
+{
+    if (F.R == 0) return false;
+    for (int64_t k = t.rank(); k < F.R; k += t.size()) {
+        const int32_t v1 = F.rr[k], v2 = F.rc[k];
+        for (int32_t e2 = F.off[v2]; e2 < F.off[v2 + 1]; ++e2) {
+            const int32_t n2 = F.c[e2];
+            for (int32_t e1 = F.off[v1]; e1 < F.off[v1 + 1]; ++e1) {
+                const int32_t n1 = F.c[e1];
+                if (n1 == n2) continue;
+                int32_t p1, p2;
+                if (first_common_pos(F, n1, n2, p1, p2) < 0) continue;
+                const float a = F.w[e1], b = F.w[e2], c1 = F.w[p1], c2 = F.w[p2];
+                int32_t cut;
+                if (a < b)
+                    cut = (a < c1 && a < c2) ? e1 : (c1 < c2 ? p1 : p2);
+                else
+                    cut = (b < c1 && b < c2) ? e2 : (c1 < c2 ? p1 : p2);
+                F.inv[cut] = 1;
+            }
+        }
+    }
+    t.sync();
+    return forest_remove_flagged(t, sc, sm, F);
+}
+
 // filter_by_thresholding (src/edge_contractions_woc_thrust.cu:522-542)
 template <class Team>
 __device__ bool forest_threshold(const Team &t, Scratch &sc, char *sm, Forest &F)
@@ -438,7 +471,7 @@ __device__ bool forest_resolve(const Team &t, Scratch &sc, char *sm, Forest &F, 
 // (0 = nothing to contract).
 template <class Team>
 __device__ int32_t woc_contraction_map(const Team &t, Scratch &sc, char *sm, const Graph &A, int32_t *map_out,
-                                       int32_t *map_size, int *err)
+                                       int32_t *map_size, int *err, bool pentagons = false)
 {
     Forest F;
     F.nn = A.max_dim();
@@ -512,6 +545,7 @@ __device__ int32_t woc_contraction_map(const Team &t, Scratch &sc, char *sm, con
     forest_filter_by_cc(t, sc, sm, F);
     if (forest_check_triangles(t, sc, sm, F)) forest_filter_by_cc(t, sc, sm, F);
     forest_check_quadrangles(t, sc, sm, F);
+    if (pentagons) forest_check_pentagons(t, sc, sm, F);  // the commented-out call at :414
     if (F.m2 == 0) {
         sc.arena.release(mark);
         return 0;

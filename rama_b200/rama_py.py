@@ -51,6 +51,7 @@ class multicut_solver_options:  # noqa: N801 (reference name)
         self.dump_timeline = False
         self.verbose = True
         self.sanitize_graph = False
+        self.woc_pentagons = False  # not in the reference: see rama_options.woc_pentagons
         if len(args) == 1 and isinstance(args[0], str):
             mode = args[0]
             if mode in _MESSAGES:
@@ -83,6 +84,7 @@ class multicut_solver_options:  # noqa: N801 (reference name)
         o.verbose = int(bool(self.verbose))
         o.sanitize_graph = int(bool(self.sanitize_graph))
         o.team = int(getattr(self, "team", team))
+        o.woc_pentagons = int(bool(self.woc_pentagons))
         return o
 
     def get_string(self):

@@ -145,9 +145,9 @@ class Solver:
         k = a.out_n
         return r[:k].cpu().numpy(), co[:k].cpu().numpy(), w[:k].cpu().numpy(), a.out_rows, a.out_cols
 
-    def _map_step(self, op, row, col, cost, rows, cols, team, mm=0.05):
+    def _map_step(self, op, row, col, cost, rows, cols, team, mm=0.05, max_cycle_length=0):
         torch = _torch()
-        a = _lib.StepArgs(op=_lib.STEP[op], team=team, mean_multiplier_mm=mm)
+        a = _lib.StepArgs(op=_lib.STEP[op], team=team, mean_multiplier_mm=mm, max_cycle_length=max_cycle_length)
         keep = []
         self._graph_args(a, row, col, cost, rows, cols, keep)
         cap = max(rows, cols) + 2
@@ -160,8 +160,9 @@ class Solver:
     def step_matching(self, row, col, cost, rows, cols, mm=0.05, team=1):
         return self._map_step("MATCHING", row, col, cost, rows, cols, team, mm)
 
-    def step_woc(self, row, col, cost, rows, cols, team=1):
-        return self._map_step("WOC", row, col, cost, rows, cols, team)
+    def step_woc(self, row, col, cost, rows, cols, team=1, pentagons=False):
+        """Forest contraction map; `pentagons` adds the 5-cycle forest check."""
+        return self._map_step("WOC", row, col, cost, rows, cols, team, max_cycle_length=5 if pentagons else 0)
 
     def step_msf(self, i, j, w, team=1):
         torch = _torch()

@@ -33,6 +33,17 @@ def test_solve_matches_oracle(solver, oracle, case, mode, team):
     assert np.array_equal(glab, olab)
 
 
+@pytest.mark.parametrize("team", (1, 2, 3))
+@pytest.mark.parametrize("case", CASES, ids=IDS)
+def test_solve_with_pentagon_check_matches_oracle(solver, oracle, case, team):
+    """woc_pentagons = 1: forest contractions also cut conflicted 5-cycles."""
+    _, (i, j, c) = case
+    olab, olb, _ = oracle.solve(i, j, c, "P", woc_pentagons=1)
+    glab, glb, _ = solver.solve(i, j, c, mode="P", team=team, woc_pentagons=1)
+    assert glb == olb
+    assert np.array_equal(glab, olab)
+
+
 @pytest.mark.parametrize("case", CASES[-3:], ids=IDS[-3:])
 def test_bound_below_objective(solver, oracle, case):
     _, (i, j, c) = case

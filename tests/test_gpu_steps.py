@@ -94,6 +94,18 @@ def test_woc(solver, oracle, g, team):
 
 
 @pytest.mark.parametrize("team", TEAMS)
+@pytest.mark.parametrize("g", GRAPHS, ids=IDS)
+def test_woc_pentagons(solver, oracle, g, team):
+    """The optional 5-cycle forest check gives the oracle's map too."""
+    _, i, j, c = g
+    G, r, co, w, rows, cols = _G(oracle, i, j, c)
+    om, onr = oracle.woc(G, pentagons=True)
+    gm, gnr = solver.step_woc(r, co, w, rows, cols, team=team, pentagons=True)
+    assert gnr == onr
+    assert np.array_equal(gm, om)
+
+
+@pytest.mark.parametrize("team", TEAMS)
 @pytest.mark.parametrize("seed", range(4))
 def test_cc(solver, oracle, seed, team):
     rng = np.random.default_rng(1200 + seed)

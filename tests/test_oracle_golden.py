@@ -152,6 +152,29 @@ def test_fixture_matching_woc_msf(oracle, F, k):
     assert mine == ref
 
 
+WOC5 = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "ref_woc5.npz")
+
+
+def test_fixture_woc_pentagons(oracle):
+    """The optional 5-cycle forest check (the reference's check_pentagons_cuda,
+    disabled there) against the reference run with it enabled; the same
+    graphs without the check match the reference's default path."""
+    if not os.path.exists(WOC5):
+        pytest.skip("tests/golden/ref_woc5.npz not generated")
+    W = np.load(WOC5)
+    cases = sorted({k.split("/")[0] for k in W.files})
+    differ = 0
+    for g in cases:
+        G = oracle.Graph.from_sorted(W[f"{g}/row"], W[f"{g}/col"], W[f"{g}/cost"])
+        assert list(G.dims) == W[f"{g}/dims"].tolist()
+        m5, n5 = oracle.woc(G, pentagons=True)
+        m4, n4 = oracle.woc(G)
+        assert np.array_equal(m5, W[f"{g}/map5"]) and n5 == W[f"{g}/nr5"][0], g
+        assert np.array_equal(m4, W[f"{g}/map4"]) and n4 == W[f"{g}/nr4"][0], g
+        differ += not np.array_equal(W[f"{g}/map5"], W[f"{g}/map4"])
+    assert differ > 0  # the check changes the result on some of these graphs
+
+
 @pytest.mark.parametrize("k", CASES)
 @pytest.mark.parametrize("L", (3, 4, 5))
 def test_fixture_cycles(oracle, F, k, L):
