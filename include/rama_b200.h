@@ -170,6 +170,22 @@ int rama_solve_small_static(const int32_t *d_i, const int32_t *d_j, const float 
                             const rama_options *opts, int32_t *d_labels, int64_t labels_cap, int64_t *num_labels,
                             double *lb, void *stream);
 
+/* Reads MULTICUT text on the device (the reference's read_file,
+ * src/multicut_text_parser.cpp:6-31): a first line "MULTICUT" (one trailing
+ * '\r' allowed), then whitespace-separated triples "i j cost" up to the first
+ * token that is not a number of its kind (int32, int32, float rounded to
+ * nearest like strtof; a cost beyond FLT_MAX ends the input as in the
+ * reference's stream extraction).  d_text: the text in device memory.  The
+ * triples go to d_i, d_j, d_costs (capacity `cap`; (len + 1) / 6 + 1 always
+ * suffices); *num_edges receives their count.  RAMA_ERR_INVALID_ARG when the
+ * first line is not "MULTICUT". */
+int rama_parse_multicut(rama_handle h, const char *d_text, int64_t len, int32_t *d_i, int32_t *d_j, float *d_costs,
+                        int64_t cap, int64_t *num_edges, void *stream);
+/* The same with the text and the triples in host memory (the text is copied
+ * to the device, parsed there, and the triples copied back). */
+int rama_parse_multicut_host(rama_handle h, const char *text, int64_t len, int32_t *i, int32_t *j, float *costs,
+                             int64_t cap, int64_t *num_edges);
+
 int rama_get_stats(rama_handle h, rama_stats *out);
 const char *rama_last_error(void);
 

@@ -88,7 +88,8 @@ class StepArgs(C.Structure):
 # every symbol include/rama_b200.h declares
 EXPORTS = ("rama_options_init", "rama_create", "rama_destroy", "rama_solve", "rama_solve_host", "rama_get_timeline",
            "rama_solve_batch", "rama_batch_launch", "rama_batch_poll", "rama_batch_wait", "rama_get_stats",
-           "rama_last_error", "rama_objective", "rama_step", "rama_solve_small_static")
+           "rama_last_error", "rama_objective", "rama_step", "rama_solve_small_static", "rama_parse_multicut",
+           "rama_parse_multicut_host")
 
 _lib = None
 _lock = threading.Lock()
@@ -126,6 +127,8 @@ def load():
         L.rama_get_stats.argtypes = [P, C.POINTER(RamaStats)]
         L.rama_solve_small_static.argtypes = [P, P, P, i64, C.POINTER(RamaOptions), P, i64, C.POINTER(i64),
                                               C.POINTER(C.c_double), P]
+        L.rama_parse_multicut.argtypes = [P, P, i64, P, P, P, i64, C.POINTER(i64), P]
+        L.rama_parse_multicut_host.argtypes = [P, C.c_char_p, i64, P, P, P, i64, C.POINTER(i64)]
         L.rama_last_error.restype = C.c_char_p
         L.rama_objective.argtypes = [P, P, P, P, i64, P, C.POINTER(C.c_double), P]
         L.rama_step.argtypes = [P, C.POINTER(StepArgs), P]

@@ -18,7 +18,8 @@
 #include "rama_cuda.h"
 
 // MULTICUT text: a first line "MULTICUT", then "i j cost" triples until the
-// first token that does not parse.
+// first token that does not parse.  The bytes are read on the host and parsed
+// on the GPU (rama_parse_multicut_host).
 static std::tuple<std::vector<int>, std::vector<int>, std::vector<float>> read_file(const std::string &filename)
 {
     std::FILE *f = std::fopen(filename.c_str(), "rb");
@@ -30,29 +31,20 @@ static std::tuple<std::vector<int>, std::vector<int>, std::vector<float>> read_f
         while ((k = std::fread(tmp, 1, sizeof(tmp), f)) > 0) buf.append(tmp, k);
         std::fclose(f);
     }
-    size_t nl = buf.find('\n');
-    std::string first = buf.substr(0, nl == std::string::npos ? buf.size() : nl);
-    if (!first.empty() && first.back() == '\r') first.pop_back();
-    if (first != "MULTICUT") throw std::runtime_error("first line must be 'MULTICUT'");
-    std::vector<int> iv, jv;
-    std::vector<float> cv;
-    const char *p = buf.c_str() + (nl == std::string::npos ? buf.size() : nl + 1);
-    for (;;) {
-        char *e;
-        errno = 0;
-        long a = std::strtol(p, &e, 10);
-        if (e == p) break;
-        p = e;
-        long b = std::strtol(p, &e, 10);
-        if (e == p) break;
-        p = e;
-        float c = std::strtof(p, &e);
-        if (e == p) break;
-        p = e;
-        iv.push_back((int)a);
-        jv.push_back((int)b);
-        cv.push_back(c);
-    }
+    const int64_t len = (int64_t)buf.size();
+    const int64_t cap = (len + 1) / 6 + 1;
+    std::vector<int> iv((size_t)cap), jv((size_t)cap);
+    std::vector<float> cv((size_t)cap);
+    rama_handle h = nullptr;
+    if (rama_create(0, 0, &h) != RAMA_OK) throw std::runtime_error(rama_last_error());
+    int64_t n = 0;
+    const int rc = rama_parse_multicut_host(h, buf.data(), len, iv.data(), jv.data(), cv.data(), cap, &n);
+    const std::string msg = rc ? rama_last_error() : "";
+    rama_destroy(h);
+    if (rc) throw std::runtime_error(msg);
+    iv.resize((size_t)n);
+    jv.resize((size_t)n);
+    cv.resize((size_t)n);
     return {iv, jv, cv};
 }
 

@@ -18,6 +18,7 @@
 #include <vector>
 
 #include "../../include/rama_b200.h"
+#include "parse.cuh"
 #include "solver.cuh"
 
 using namespace rama;
@@ -127,6 +128,29 @@ struct GridLaunch {
     char *ws;
     uint64_t ws_bytes;
 };
+
+// MULTICUT text -> triples on the cooperative grid
+struct ParseLaunch {
+    const char *text;
+    int64_t len;
+    int32_t *i, *j;
+    float *c;
+    int64_t cap;
+    int64_t *out;  // count, -1 bad first line, -2 workspace exhausted
+    char *ws;
+    uint64_t ws_bytes;
+};
+
+__global__ void __launch_bounds__(THREADS, 2) k_parse_grid(ParseLaunch L)
+{
+    extern __shared__ __align__(16) char sm[];
+    GridTeam t;
+    Scratch sc = make_scratch(L.ws, L.ws_bytes);
+    if (t.rank() == 0) *sc.err = 0;
+    t.sync();
+    const int64_t n = parse_multicut(t, sc, sm, L.text, L.len, L.i, L.j, L.c, L.cap);
+    if (t.leader()) L.out[0] = sc.arena.ok() ? n : -2;
+}
 
 __global__ void __launch_bounds__(THREADS, 2) k_solve_grid(GridLaunch L)
 {
@@ -370,6 +394,9 @@ struct rama_context {
     int obj_ctas = 0;   // ... of k_objective
     int cta_per_sm = 0;
     int cluster_max = 0;  // co-resident clusters of k_solve_mixed
+    int parse_ctas = 0;   // co-resident CTAs of k_parse_grid
+    char *p_text = nullptr;  // device copy of text for rama_parse_multicut_host
+    int64_t p_cap = 0;
     char *ws = nullptr;
     uint64_t ws_bytes = 0;
     uint64_t ws_fixed = 0;  // user-requested size (0 = automatic)
@@ -640,7 +667,8 @@ int rama_create(int device, uint64_t workspace_bytes, rama_handle *out)
     h->sms = p.multiProcessorCount;
     // the sort stages a tile in shared memory: more than the default 48 KB
     for (const void *k : {(const void *)k_solve_grid, (const void *)k_solve_cta, (const void *)k_solve_mixed,
-                          (const void *)k_step_grid, (const void *)k_step_cta, (const void *)k_objective})
+                          (const void *)k_step_grid, (const void *)k_step_cta, (const void *)k_objective,
+                          (const void *)k_parse_grid})
         CU(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM));
     int per_sm = 0;
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_solve_grid, THREADS, SMEM));
@@ -653,6 +681,8 @@ int rama_create(int device, uint64_t workspace_bytes, rama_handle *out)
     h->step_ctas = std::max(1, per_sm) * h->sms;
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_objective, THREADS, SMEM));
     h->obj_ctas = std::max(1, per_sm) * h->sms;
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_parse_grid, THREADS, SMEM));
+    h->parse_ctas = std::max(1, per_sm) * h->sms;
     int per_sm_cta = 0;
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_cta, k_solve_cta, THREADS, SMEM));
     h->cta_per_sm = std::max(1, per_sm_cta);
@@ -699,6 +729,7 @@ void rama_destroy(rama_handle h)
     cudaFree(h->io_j);
     cudaFree(h->io_c);
     cudaFree(h->io_l);
+    cudaFree(h->p_text);
     cudaEventDestroy(h->ev0);
     cudaEventDestroy(h->ev1);
     cudaEventDestroy(h->ev_done);
@@ -957,6 +988,71 @@ int rama_get_stats(rama_handle h, rama_stats *out)
 {
     if (!h || !out) return fail(RAMA_ERR_INVALID_ARG, "bad arguments");
     *out = h->stats;
+    return RAMA_OK;
+}
+
+int rama_parse_multicut(rama_handle h, const char *d_text, int64_t len, int32_t *d_i, int32_t *d_j, float *d_costs,
+                        int64_t cap, int64_t *num_edges, void *stream)
+{
+    if (!h || len < 0 || (len > 0 && !d_text) || cap < 0 || (cap > 0 && (!d_i || !d_j || !d_costs)) || !num_edges)
+        return fail(RAMA_ERR_INVALID_ARG, "bad arguments");
+    CU(cudaSetDevice(h->device));
+    cudaStream_t st = (cudaStream_t)stream;
+    // tokens: 8 + 4 bytes for at most len / 2 of them, plus the scratch partials
+    int rc = ensure_ws(h, std::max<uint64_t>(h->ws_bytes, (uint64_t)len * 7 + (64ull << 20)));
+    if (rc) return rc;
+    if (h->ws_bytes < (uint64_t)len * 7 + (4ull << 20)) return fail(RAMA_ERR_OOM, "workspace too small for the text");
+    int64_t *d_out = reinterpret_cast<int64_t *>(h->d_scalar);
+    ParseLaunch L{d_text, len, d_i, d_j, d_costs, cap, d_out, h->ws, h->ws_bytes};
+    void *args[] = {&L};
+    CU(cudaLaunchCooperativeKernel((void *)k_parse_grid, dim3(h->parse_ctas), dim3(THREADS), args, SMEM, st));
+    int64_t n = 0;
+    CU(cudaMemcpyAsync(&n, d_out, sizeof(int64_t), cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    if (n == -1) return fail(RAMA_ERR_INVALID_ARG, "first line must be 'MULTICUT'");
+    if (n < 0) return fail(RAMA_ERR_OOM, "workspace too small for the text");
+    *num_edges = n;
+    return RAMA_OK;
+}
+
+int rama_parse_multicut_host(rama_handle h, const char *text, int64_t len, int32_t *i, int32_t *j, float *costs,
+                             int64_t cap, int64_t *num_edges)
+{
+    if (!h || len < 0 || (len > 0 && !text) || cap < 0 || (cap > 0 && (!i || !j || !costs)) || !num_edges)
+        return fail(RAMA_ERR_INVALID_ARG, "bad arguments");
+    CU(cudaSetDevice(h->device));
+    if (h->p_cap < std::max<int64_t>(len, 1)) {
+        cudaFree(h->p_text);
+        h->p_text = nullptr;
+        h->p_cap = 0;
+        CU(cudaMalloc(&h->p_text, (size_t)std::max<int64_t>(len, 1)));
+        h->p_cap = std::max<int64_t>(len, 1);
+    }
+    const int64_t room = std::max<int64_t>(std::min<int64_t>(cap, (len + 1) / 6 + 1), 1);
+    if (h->io_edges < room) {
+        cudaFree(h->io_i);
+        cudaFree(h->io_j);
+        cudaFree(h->io_c);
+        h->io_i = h->io_j = nullptr;
+        h->io_c = nullptr;
+        h->io_edges = 0;
+        CU(cudaMalloc(&h->io_i, sizeof(int32_t) * (size_t)room));
+        CU(cudaMalloc(&h->io_j, sizeof(int32_t) * (size_t)room));
+        CU(cudaMalloc(&h->io_c, sizeof(float) * (size_t)room));
+        h->io_edges = room;
+    }
+    cudaStream_t st = nullptr;
+    if (len > 0) CU(cudaMemcpyAsync(h->p_text, text, (size_t)len, cudaMemcpyHostToDevice, st));
+    int64_t n = 0;
+    int rc = rama_parse_multicut(h, h->p_text, len, h->io_i, h->io_j, h->io_c, room, &n, st);
+    if (rc) return rc;
+    if (n > cap) n = cap;
+    if (n > 0) {
+        CU(cudaMemcpy(i, h->io_i, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToHost));
+        CU(cudaMemcpy(j, h->io_j, sizeof(int32_t) * (size_t)n, cudaMemcpyDeviceToHost));
+        CU(cudaMemcpy(costs, h->io_c, sizeof(float) * (size_t)n, cudaMemcpyDeviceToHost));
+    }
+    *num_edges = n;
     return RAMA_OK;
 }
 

@@ -89,6 +89,23 @@ class Solver:
         out = [(lab[lo[k]:lo[k] + nl[k]].copy(), float(lbs[k])) for k in range(batch.count)]
         return out, st, rc
 
+    def parse_multicut(self, text: bytes, stream=None):
+        """MULTICUT text (bytes) parsed on the device: (i, j, costs) as device tensors."""
+        torch = _torch()
+        n = len(text)
+        d_text = torch.frombuffer(bytearray(text), dtype=torch.uint8).cuda() if n else torch.empty(1, dtype=torch.uint8,
+                                                                                                   device="cuda")
+        cap = (n + 1) // 6 + 1
+        d_i = torch.empty(cap, dtype=torch.int32, device="cuda")
+        d_j = torch.empty(cap, dtype=torch.int32, device="cuda")
+        d_c = torch.empty(cap, dtype=torch.float32, device="cuda")
+        ne = C.c_int64(0)
+        st = stream if stream is not None else C.c_void_p(torch.cuda.current_stream().cuda_stream)
+        _lib.check(_lib.load().rama_parse_multicut(self.handle.h, _p(d_text), n, _p(d_i), _p(d_j), _p(d_c), cap,
+                                                   C.byref(ne), st))
+        k = ne.value
+        return d_i[:k], d_j[:k], d_c[:k]
+
     def objective(self, d_i, d_j, d_c, d_labels):
         obj = C.c_double(0)
         torch = _torch()
