@@ -59,26 +59,61 @@ __device__ int64_t tri_normalize(const Team &t, Scratch &sc, char *sm, int32_t *
     uint64_t m = sc.arena.mark();
     uint64_t *k1 = sc.arena.take<uint64_t>(n + 1), *k2 = sc.arena.take<uint64_t>(n + 1);
     uint64_t *u1 = sc.arena.take<uint64_t>(n + 1), *u2 = sc.arena.take<uint64_t>(n + 1);
+    int32_t *tlo = sc.arena.take<int32_t>(n + 1);
     if (!sc.arena.ok()) return 0;
-    // stable sort by t3 carrying (t1,t2); then by (t1,t2) carrying t3
+    const uint64_t mask = (nb == 0) ? 0 : ((uint64_t(1) << nb) - 1);
+    // drop degenerate triangles; key the rest by lo and (md, hi)
     const int64_t w = team_compact(
         t, sc, sm, n, [&](int64_t k) { return !(t1[k] == t2[k] || t1[k] == t3[k] || t2[k] == t3[k]); },
         [&](int64_t k, int64_t p) {
             int32_t a = t1[k], b = t2[k], c = t3[k];
             int32_t lo = min(a, min(b, c)), hi = max(a, max(b, c));
             int32_t md = max(min(a, b), min(max(a, b), c));
-            k1[p] = (uint64_t)(uint32_t)hi;
-            u1[p] = pack_key(lo, md, nb);
+            tlo[p] = lo;
+            u1[p] = pack_key(md, hi, nb);
         });
-    team_sort_pairs(t, sc, sm, k1, u1, k2, u2, w, nb);
-    for (int64_t k = t.rank(); k < w; k += t.size()) {
-        uint64_t tmp = u1[k];
-        u1[k] = k1[k];  // t3 becomes the value
-        k1[k] = tmp;
+    // sort by (lo, md, hi): bucket by lo (identical triangles may end in any
+    // order among themselves, they are merged below) ...
+    bool done = false;
+    {
+        uint64_t bm = sc.arena.mark();
+        int32_t *bst = sc.arena.take<int32_t>((int64_t)nmax + 2);
+        int32_t *bidx = sc.arena.take<int32_t>(w + 1);
+        if (sc.arena.ok() && w < (int64_t(1) << 31)) {
+            done = team_bucket_sort(
+                t, sc, sm, w, nmax + 1, [&](int64_t i) { return tlo[i]; }, [&](int64_t i) { return u1[i]; }, k2, bidx,
+                bst);
+            if (done) {
+                for (int64_t b = t.rank(); b <= nmax; b += t.size())
+                    for (int32_t p = bst[b]; p < bst[b + 1]; ++p) {
+                        k1[p] = pack_key((int32_t)b, (int32_t)(k2[p] >> nb), nb);
+                        u2[p] = k2[p] & mask;
+                    }
+                t.sync();
+                uint64_t *tp = u1;
+                u1 = u2;
+                u2 = tp;
+            }
+        }
+        sc.arena.release(bm);
     }
-    t.sync();
-    team_sort_pairs(t, sc, sm, k1, u1, k2, u2, w, 2 * nb);
-    const uint64_t mask = (nb == 0) ? 0 : ((uint64_t(1) << nb) - 1);
+    if (!done) {
+        // ... or by LSD radix: stable sort by hi carrying (lo, md), then by (lo, md) carrying hi
+        for (int64_t k = t.rank(); k < w; k += t.size()) {
+            const uint64_t mh = u1[k];
+            k1[k] = mh & mask;
+            u1[k] = pack_key(tlo[k], (int32_t)(mh >> nb), nb);
+        }
+        t.sync();
+        team_sort_pairs(t, sc, sm, k1, u1, k2, u2, w, nb);
+        for (int64_t k = t.rank(); k < w; k += t.size()) {
+            uint64_t tmp = u1[k];
+            u1[k] = k1[k];  // hi becomes the value
+            k1[k] = tmp;
+        }
+        t.sync();
+        team_sort_pairs(t, sc, sm, k1, u1, k2, u2, w, 2 * nb);
+    }
     const int64_t u = team_compact(
         t, sc, sm, w, [&](int64_t k) { return k == 0 || k1[k] != k1[k - 1] || u1[k] != u1[k - 1]; },
         [&](int64_t k, int64_t p) {
@@ -91,9 +126,23 @@ __device__ int64_t tri_normalize(const Team &t, Scratch &sc, char *sm, int32_t *
 }
 
 // Expansion stage over X expansions (X given as an exclusive scan xo[R+1]
-// over rep edges).  For each expansion: count(x) emissions, then write them
-// at `count + prefix`.  Processed in chunks so that a filled budget stops the
-// work early.
+// over rep edges; xo == nullptr means one expansion per rep edge).  For each
+// expansion: count(x) emissions, then write them at `count + prefix`.
+// Processed in chunks so that a filled budget stops the work early.
+__device__ __forceinline__ int64_t expansion_owner(const int64_t *xo, int64_t R, int64_t x)
+{
+    if (!xo) return x;
+    int64_t lo = 0, hi = R;  // largest r with xo[r] <= x
+    while (lo < hi) {
+        int64_t mid = (lo + hi + 1) >> 1;
+        if (xo[mid] <= x)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
 template <class Team, class Count, class Emit>
 __device__ void expansion_stage(const Team &t, Scratch &sc, char *sm, TriBuf &tb, const int64_t *xo, int64_t R,
                                 int64_t X, Count cnt, Emit emit)
@@ -107,16 +156,9 @@ __device__ void expansion_stage(const Team &t, Scratch &sc, char *sm, TriBuf &tb
         const int64_t xn = (X - x0) < CH ? (X - x0) : CH;
         // count
         for (int64_t q = t.rank(); q < xn; q += t.size()) {
-            int64_t x = x0 + q;
-            int64_t lo = 0, hi = R;  // largest r with xo[r] <= x
-            while (lo < hi) {
-                int64_t mid = (lo + hi + 1) >> 1;
-                if (xo[mid] <= x)
-                    lo = mid;
-                else
-                    hi = mid - 1;
-            }
-            ccount[q] = cnt(lo, x - xo[lo]);
+            const int64_t x = x0 + q;
+            const int64_t r = expansion_owner(xo, R, x);
+            ccount[q] = cnt(r, xo ? x - xo[r] : 0);
         }
         t.sync();
         const int64_t tot = team_scan<Team, int64_t>(
@@ -125,16 +167,9 @@ __device__ void expansion_stage(const Team &t, Scratch &sc, char *sm, TriBuf &tb
         const int64_t start = tb.count;
         for (int64_t q = t.rank(); q < xn; q += t.size()) {
             if (ccount[q] == 0 || start + cbase[q] >= tb.budget) continue;
-            int64_t x = x0 + q;
-            int64_t lo = 0, hi = R;
-            while (lo < hi) {
-                int64_t mid = (lo + hi + 1) >> 1;
-                if (xo[mid] <= x)
-                    lo = mid;
-                else
-                    hi = mid - 1;
-            }
-            emit(lo, x - xo[lo], start + cbase[q]);
+            const int64_t x = x0 + q;
+            const int64_t r = expansion_owner(xo, R, x);
+            emit(r, xo ? x - xo[r] : 0, start + cbase[q]);
         }
         t.sync();
         tb.count = start + tot;
@@ -178,11 +213,9 @@ __device__ void conflicted_cycles(const Team &t, Scratch &sc, char *sm, const Gr
     auto rv2 = [&](int64_t r) { return A.col[ridx[r]]; };
     // ---- 3-cycles: find_triangles_parallel (:31-61)
     {
-        for (int64_t r = t.rank(); r <= R; r += t.size()) xo[r] = r;
-        t.sync();
         TriBuf &T = tb;
         expansion_stage(
-            t, sc, sm, T, xo, R, R,
+            t, sc, sm, T, nullptr, R, R,
             [&](int64_t r, int64_t) {
                 int32_t v1 = rv1(r), v2 = rv2(r);
                 return count_common(adj, off[v1], off[v1 + 1], off[v2], off[v2 + 1]);

@@ -91,13 +91,40 @@ __device__ Graph graph_from_edges(const Team &t, Scratch &sc, char *sm, const in
     float *v1 = sc.arena.take<float>(n + 1), *v2 = sc.arena.take<float>(n + 1);
     Graph g = graph_alloc(t, sc, n);
     if (!sc.arena.ok()) return out;
-    for (int64_t e = t.rank(); e < n; e += t.size()) {
-        int32_t a = i[e], b = j[e];
-        k1[e] = pack_key(a < b ? a : b, a < b ? b : a, nb);
-        v1[e] = c[e];
+    // sort by (min, max) endpoint, stably: bucket by the smaller endpoint and
+    // order each bucket by (larger endpoint, edge index); hub rows of more
+    // than BUCKET_MAX edges: LSD radix sort
+    bool done = false;
+    {
+        uint64_t bm = sc.arena.mark();
+        int32_t *bst = sc.arena.take<int32_t>((int64_t)mx + 2);
+        int32_t *bidx = sc.arena.take<int32_t>(n + 1);
+        if (sc.arena.ok() && n < (int64_t(1) << 31)) {
+            done = team_bucket_sort(
+                t, sc, sm, n, mx + 1, [&](int64_t e) { return i[e] < j[e] ? i[e] : j[e]; },
+                [&](int64_t e) -> uint64_t {
+                    return ((uint64_t)(uint32_t)(i[e] < j[e] ? j[e] : i[e]) << 32) | (uint64_t)e;
+                },
+                k2, bidx, bst);
+            if (done) {
+                for (int64_t b = t.rank(); b <= mx; b += t.size())
+                    for (int32_t p = bst[b]; p < bst[b + 1]; ++p)
+                        k1[p] = pack_key((int32_t)b, (int32_t)(k2[p] >> 32), nb);
+                for (int64_t p = t.rank(); p < n; p += t.size()) v1[p] = c[bidx[p]];
+                t.sync();
+            }
+        }
+        sc.arena.release(bm);
     }
-    t.sync();
-    team_sort_pairs(t, sc, sm, k1, v1, k2, v2, n, 2 * nb);
+    if (!done) {
+        for (int64_t e = t.rank(); e < n; e += t.size()) {
+            int32_t a = i[e], b = j[e];
+            k1[e] = pack_key(a < b ? a : b, a < b ? b : a, nb);
+            v1[e] = c[e];
+        }
+        t.sync();
+        team_sort_pairs(t, sc, sm, k1, v1, k2, v2, n, 2 * nb);
+    }
     const uint64_t mask = (nb == 0) ? 0 : ((uint64_t(1) << nb) - 1);
     for (int64_t e = t.rank(); e < n; e += t.size()) {
         g.row[e] = (int32_t)(k1[e] >> nb);
@@ -118,6 +145,52 @@ __device__ Graph graph_from_edges(const Team &t, Scratch &sc, char *sm, const in
 // Returns the new graph (committed to the top slot); *bad is set if a
 // self-loop of negative cost appeared.  Dims are taken before the diagonal
 // is removed, as the reference does.
+// The edges keyed by their contracted endpoints, sorted: k1[p] = (lo, hi)
+// packed with nb bits each, v1[p] = the edge's cost, in (lo, hi) order and,
+// for equal keys, in edge order (the order a stable sort leaves; it fixes the
+// summation order of parallel edges).  The edges are bucketed by their new
+// row lo and each row is ordered by (hi, edge index); rows of more than
+// BUCKET_MAX edges send the whole list through the LSD radix sort instead.
+// k1/v1 (and the spare k2/v2) hold n + 1 entries; the result ends in k1/v1.
+template <class Team>
+__device__ void contract_sorted_keys(const Team &t, Scratch &sc, char *sm, const Graph &A, const int32_t *map,
+                                     int32_t map_max, int nb, uint64_t *&k1, float *&v1, uint64_t *&k2, float *&v2)
+{
+    const int64_t n = A.n;
+    bool done = false;
+    uint64_t m = sc.arena.mark();
+    int32_t *bst = sc.arena.take<int32_t>((int64_t)map_max + 2);
+    int32_t *bidx = sc.arena.take<int32_t>(n + 1);
+    if (sc.arena.ok() && n < (int64_t(1) << 31)) {
+        done = team_bucket_sort(
+            t, sc, sm, n, map_max + 1,
+            [&](int64_t e) {
+                const int32_t a = map[A.row[e]], b = map[A.col[e]];
+                return a < b ? a : b;
+            },
+            [&](int64_t e) -> uint64_t {
+                const int32_t a = map[A.row[e]], b = map[A.col[e]];
+                return ((uint64_t)(uint32_t)(a < b ? b : a) << 32) | (uint64_t)e;
+            },
+            k2, bidx, bst);
+        if (done) {
+            for (int64_t b = t.rank(); b <= map_max; b += t.size())
+                for (int32_t p = bst[b]; p < bst[b + 1]; ++p) k1[p] = pack_key((int32_t)b, (int32_t)(k2[p] >> 32), nb);
+            for (int64_t p = t.rank(); p < n; p += t.size()) v1[p] = A.cost[bidx[p]];
+            t.sync();
+        }
+    }
+    sc.arena.release(m);
+    if (done) return;
+    for (int64_t e = t.rank(); e < n; e += t.size()) {
+        int32_t a = map[A.row[e]], b = map[A.col[e]];
+        k1[e] = pack_key(a < b ? a : b, a < b ? b : a, nb);
+        v1[e] = A.cost[e];
+    }
+    t.sync();
+    team_sort_pairs(t, sc, sm, k1, v1, k2, v2, n, 2 * nb);
+}
+
 template <class Team>
 __device__ Graph graph_contract(const Team &t, Scratch &sc, char *sm, const Graph &A, const int32_t *map,
                                 int32_t map_max, int *bad)
@@ -131,14 +204,8 @@ __device__ Graph graph_contract(const Team &t, Scratch &sc, char *sm, const Grap
     int32_t *badflag = sc.arena.take<int32_t>(2);
     Graph out = A;
     if (!sc.arena.ok()) return out;
-    for (int64_t e = t.rank(); e < n; e += t.size()) {
-        int32_t a = map[A.row[e]], b = map[A.col[e]];
-        k1[e] = pack_key(a < b ? a : b, a < b ? b : a, nb);
-        v1[e] = A.cost[e];
-    }
     if (t.rank() == 0) badflag[0] = 0;
-    t.sync();
-    team_sort_pairs(t, sc, sm, k1, v1, k2, v2, n, 2 * nb);
+    contract_sorted_keys(t, sc, sm, A, map, map_max, nb, k1, v1, k2, v2);
     // run heads -> run index
     const int64_t nruns = team_compact(
         t, sc, sm, n, [&](int64_t k) { return k == 0 || k1[k] != k1[k - 1]; },
@@ -261,13 +328,7 @@ __device__ Graph graph_contract_raw(const Team &t, Scratch &sc, char *sm, const 
     int64_t *runpos = sc.arena.take<int64_t>(n + 2);
     Graph out = A;
     if (!sc.arena.ok()) return out;
-    for (int64_t e = t.rank(); e < n; e += t.size()) {
-        int32_t a = map[A.row[e]], b = map[A.col[e]];
-        k1[e] = pack_key(a < b ? a : b, a < b ? b : a, nb);
-        v1[e] = A.cost[e];
-    }
-    t.sync();
-    team_sort_pairs(t, sc, sm, k1, v1, k2, v2, n, 2 * nb);
+    contract_sorted_keys(t, sc, sm, A, map, map_max, nb, k1, v1, k2, v2);
     const int64_t nruns = team_compact(
         t, sc, sm, n, [&](int64_t k) { return k == 0 || k1[k] != k1[k - 1]; },
         [&](int64_t k, int64_t r) { runpos[r] = k; });
@@ -362,16 +423,35 @@ __device__ Csr build_symmetric_csr(const Team &t, Scratch &sc, char *sm, const G
         [&](int64_t v, int64_t pre, int64_t) { rowstart[v] = (int32_t)pre; });
     if (t.rank() == 0) C.off[nrows] = (int32_t)(2 * m);
     t.sync();
-    // 3. stable sort of kept edges by column -> reverse entries in increasing row order
-    team_sort_pairs(t, sc, sm, k1, v1, k2, v2, m, bits_for((uint64_t)(nrows > 0 ? nrows : 1)));
-    for (int64_t q = t.rank(); q < m; q += t.size()) {
-        int32_t c = (int32_t)k1[q];
-        int64_t p = v1[q];
-        int64_t e = kidx[p];
-        int64_t dst = (int64_t)C.off[c] + (q - colstart[c]);
-        C.adj[dst] = A.row[e];
-        C.w[dst] = A.cost[e];
-        if (with_eid) C.eid[dst] = (int32_t)p;
+    // 3. kept edges in column order, rows increasing within a column (a
+    //    bucket sort by column of the kept positions, which are in row order;
+    //    columns of more than BUCKET_MAX entries: a stable radix sort) ->
+    //    the reverse entries
+    int32_t *bst = sc.arena.take<int32_t>((int64_t)nrows + 2);
+    if (sc.arena.ok() && m < (int64_t(1) << 31) &&
+        team_bucket_sort(
+            t, sc, sm, m, nrows, [&](int64_t p) { return A.col[kidx[p]]; }, [&](int64_t p) { return (uint64_t)p; },
+            k2, v2, bst)) {
+        for (int64_t q = t.rank(); q < m; q += t.size()) {
+            const int64_t p = (int64_t)k2[q];
+            const int64_t e = kidx[p];
+            const int32_t c = A.col[e];
+            const int64_t dst = (int64_t)C.off[c] + (q - bst[c]);
+            C.adj[dst] = A.row[e];
+            C.w[dst] = A.cost[e];
+            if (with_eid) C.eid[dst] = (int32_t)p;
+        }
+    } else {
+        team_sort_pairs(t, sc, sm, k1, v1, k2, v2, m, bits_for((uint64_t)(nrows > 0 ? nrows : 1)));
+        for (int64_t q = t.rank(); q < m; q += t.size()) {
+            int32_t c = (int32_t)k1[q];
+            int64_t p = v1[q];
+            int64_t e = kidx[p];
+            int64_t dst = (int64_t)C.off[c] + (q - colstart[c]);
+            C.adj[dst] = A.row[e];
+            C.w[dst] = A.cost[e];
+            if (with_eid) C.eid[dst] = (int32_t)p;
+        }
     }
     // forward entries: the kept edges of row r are contiguous in kidx order
     for (int64_t p = t.rank(); p < m; p += t.size()) {

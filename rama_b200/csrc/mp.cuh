@@ -95,7 +95,27 @@ __device__ bool mp_build(const Team &t, Scratch &sc, char *sm, const Graph &A, T
             nk1[p] = pack_key(a, b, nb);
             nv1[p] = 0;
         });
-    team_sort_pairs(t, sc, sm, nk1, nv1, nk2, nv2, nn, 2 * nb);
+    {
+        // sort the chords (a, b): bucket by a, order by b (equal chords are
+        // merged below, so their order does not matter); rows of more than
+        // BUCKET_MAX chords: LSD radix sort
+        const uint64_t cmask = (nb == 0) ? 0 : ((uint64_t(1) << nb) - 1);
+        uint64_t bm = sc.arena.mark();
+        int32_t *bst = sc.arena.take<int32_t>((int64_t)nmax + 2);
+        bool done = false;
+        if (sc.arena.ok() && nn < (int64_t(1) << 31)) {
+            done = team_bucket_sort(
+                t, sc, sm, nn, nmax + 1, [&](int64_t q) { return (int32_t)(nk1[q] >> nb); },
+                [&](int64_t q) { return nk1[q] & cmask; }, nk2, nv2, bst);
+            if (done) {
+                for (int64_t b = t.rank(); b <= nmax; b += t.size())
+                    for (int32_t p = bst[b]; p < bst[b + 1]; ++p) nk1[p] = ((uint64_t)b << nb) | nk2[p];
+                t.sync();
+            }
+        }
+        sc.arena.release(bm);
+        if (!done) team_sort_pairs(t, sc, sm, nk1, nv1, nk2, nv2, nn, 2 * nb);
+    }
     uint64_t *nu = nk2;  // unique chords
     const int64_t nu_n = team_compact(
         t, sc, sm, nn, [&](int64_t k) { return k == 0 || nk1[k] != nk1[k - 1]; },
@@ -164,13 +184,21 @@ __device__ bool mp_build(const Team &t, Scratch &sc, char *sm, const Graph &A, T
         w1[3 * k + 2] = (int32_t)(3 * k + 2);
     }
     t.sync();
-    // incidence order: stable sort of (edge, 3t + corner) by edge; the rank of
-    // each (triangle, corner) in that order is its slot
-    int32_t *incp = w1;
-    uint64_t *qk = q1;
-    team_sort_pairs(t, sc, sm, qk, incp, q2, w2, 3 * T, bits_for((uint64_t)(E > 0 ? E : 1)));
-    for (int64_t q = t.rank(); q < 3 * T; q += t.size()) mp.pos[incp[q]] = (int32_t)q;
-    team_offsets(t, 3 * T, (int32_t)E, [&](int64_t k) { return (int32_t)qk[k]; }, mp.inc_off);
+    // incidence order: (edge, 3t + corner) sorted by edge, then by 3t + corner;
+    // the rank of each (triangle, corner) in that order is its slot
+    if (3 * T < (int64_t(1) << 31) &&
+        team_bucket_sort(
+            t, sc, sm, 3 * T, (int32_t)E, [&](int64_t q) { return (int32_t)q1[q]; },
+            [&](int64_t q) { return (uint64_t)q; }, q2, w2, mp.inc_off)) {
+        for (int64_t q = t.rank(); q < 3 * T; q += t.size()) mp.pos[w2[q]] = (int32_t)q;
+        t.sync();
+    } else {
+        int32_t *incp = w1;
+        uint64_t *qk = q1;
+        team_sort_pairs(t, sc, sm, qk, incp, q2, w2, 3 * T, bits_for((uint64_t)(E > 0 ? E : 1)));
+        for (int64_t q = t.rank(); q < 3 * T; q += t.size()) mp.pos[incp[q]] = (int32_t)q;
+        team_offsets(t, 3 * T, (int32_t)E, [&](int64_t k) { return (int32_t)qk[k]; }, mp.inc_off);
+    }
     sc.arena.release(ik);
     // each covered edge's share of its cost, and the edges whose incoming
     // messages a whole warp sums

@@ -721,6 +721,186 @@ __host__ __device__ constexpr int sort_smem_bytes(int threads)
 }
 
 // ---------------------------------------------------------------------------
+// Bucket sort: n items ordered by (bucket(i), sub(i)), bucket(i) in [0, nb),
+// sub(i) below 2^64 - 1.  Items with equal (bucket, sub) end in no particular
+// order: callers fold the item index into sub when the order must be stable,
+// and otherwise use it only where equal keys stand for equal items.  Each item takes a slot in
+// its bucket by an atomic counter (one atomic per bucket and warp), an
+// exclusive scan of the counts gives the bucket starts, one scatter places
+// the items, and each bucket is then sorted by its sub keys: buckets of up to
+// 64 items by ranking every item (it lands after the keys of its bucket that
+// are smaller), up to 256 items by a warp and up to BUCKET_MAX by a CTA
+// (bitonic networks in shared memory).  The
+// atomic slots only decide where an item lands before its bucket is sorted,
+// so with distinct keys the result is the one sorted order.
+// Outputs: keys_out[p] = sub of the p-th item, idx_out[p] = its index,
+// bstart[0, nb] = first position of each bucket.  Returns false, having
+// written nothing useful, when a bucket holds more than BUCKET_MAX items (the
+// caller then sorts with team_sort_pairs).
+// ---------------------------------------------------------------------------
+constexpr int BUCKET_MAX = 4096;
+
+// bitonic sort of (key, idx) pairs in shared memory, `m` items padded to the
+// power of two P with +inf keys; threads [lo, lo + nth) of the group work,
+// `bar` synchronises them
+template <class Bar>
+__device__ __forceinline__ void smem_bitonic(uint64_t *key, int32_t *idx, int m, int P, int lane, int nth, Bar bar)
+{
+    for (int i = m + lane; i < P; i += nth) {
+        key[i] = ~uint64_t(0);
+        idx[i] = -1;
+    }
+    bar();
+    for (int k = 2; k <= P; k <<= 1) {
+        for (int j = k >> 1; j > 0; j >>= 1) {
+            for (int i = lane; i < P; i += nth) {
+                const int x = i ^ j;
+                if (x > i) {
+                    const uint64_t a = key[i], b = key[x];
+                    if ((a > b) == ((i & k) == 0)) {
+                        key[i] = b;
+                        key[x] = a;
+                        const int32_t t = idx[i];
+                        idx[i] = idx[x];
+                        idx[x] = t;
+                    }
+                }
+            }
+            bar();
+        }
+    }
+}
+
+template <class Team, class Bk, class Sub>
+__device__ bool team_bucket_sort(const Team &t, Scratch &sc, char *sm, int64_t n, int32_t nb, Bk bucket, Sub sub,
+                                 uint64_t *keys_out, int32_t *idx_out, int32_t *bstart)
+{
+    uint64_t am = sc.arena.mark();
+    int32_t *slot = sc.arena.take<int32_t>(n + 1);
+    int32_t *tb = sc.arena.take<int32_t>(n + 1);    // bucket of the item at each scattered position
+    int32_t *ti = sc.arena.take<int32_t>(n + 1);    // item index at each scattered position
+    uint64_t *tk = sc.arena.take<uint64_t>(n + 1);  // sub key at each scattered position
+    int32_t *lists = sc.arena.take<int32_t>(2 * ((int64_t)nb + 1));  // warp buckets, CTA buckets
+    int32_t *nlist = sc.arena.take<int32_t>(4);
+    if (!sc.arena.ok()) return false;
+    int32_t *wlist = lists, *clist = lists + nb + 1;
+    for (int64_t b = t.rank(); b <= nb; b += t.size()) bstart[b] = 0;
+    if (t.rank() < 4) nlist[t.rank()] = 0;
+    t.sync();
+    // slots: the lanes of a warp that share a bucket take theirs with one atomic
+    for (int64_t base = (int64_t)t.rank() - lane_id(); base < n; base += t.size()) {
+        const int64_t i = base + lane_id();
+        const bool valid = i < n;
+        const int32_t b = valid ? (int32_t)bucket(i) : -1;
+        const unsigned peers = __match_any_sync(FULL, b);
+        const int leader = __ffs(peers) - 1;
+        int32_t s0 = 0;
+        if (valid && lane_id() == leader) s0 = atomicAdd(&bstart[b], __popc(peers));
+        s0 = __shfl_sync(FULL, s0, leader);
+        if (valid) slot[i] = s0 + __popc(peers & lanemask_lt());
+    }
+    t.sync();
+    const int32_t big = team_max<Team, int32_t>(t, sc, sm, nb, 0, [&](int64_t b) { return bstart[b]; });
+    if (big > BUCKET_MAX) {
+        sc.arena.release(am);
+        return false;
+    }
+    // buckets of more than 64 items: the warp and CTA lists (any order)
+    for (int64_t b = t.rank(); b < nb; b += t.size()) {
+        const int32_t c = bstart[b];
+        if (c > 256)
+            clist[atomicAdd(&nlist[1], 1)] = (int32_t)b;
+        else if (c > 64)
+            wlist[atomicAdd(&nlist[0], 1)] = (int32_t)b;
+    }
+    team_scan<Team, int64_t>(
+        t, sc, sm, nb, [&](int64_t b) -> int64_t { return bstart[b]; },
+        [&](int64_t b, int64_t pre, int64_t) { bstart[b] = (int32_t)pre; });
+    if (t.rank() == 0) bstart[nb] = (int32_t)n;
+    t.sync();
+    for (int64_t i = t.rank(); i < n; i += t.size()) {
+        const int32_t b = (int32_t)bucket(i);
+        const int64_t p = (int64_t)bstart[b] + slot[i];
+        tk[p] = sub(i);
+        ti[p] = (int32_t)i;
+        tb[p] = b;
+    }
+    t.sync();
+    // up to 64 items: each item's rank in its bucket is the number of smaller
+    // keys there (neighbouring threads read the same bucket)
+    for (int64_t p = t.rank(); p < n; p += t.size()) {
+        const int32_t b = tb[p], s = bstart[b], e = bstart[b + 1];
+        if (e - s > 64) {
+            keys_out[p] = tk[p];
+            idx_out[p] = ti[p];
+            continue;
+        }
+        const uint64_t k = tk[p];
+        int32_t r = 0;
+        for (int32_t q = s; q < e; ++q) {
+            const uint64_t o = tk[q];
+            r += o < k || (o == k && q < p);
+        }
+        keys_out[s + r] = k;
+        idx_out[s + r] = ti[p];
+    }
+    t.sync();
+    // 65..256 items: a warp, bitonic in its share of the staging area
+    {
+        const int NW = blockDim.x >> 5;
+        const int w = warp_in_block();
+        char *stage = sm + NW * 1024;
+        uint64_t *wk = reinterpret_cast<uint64_t *>(stage) + w * 256;
+        int32_t *wi = reinterpret_cast<int32_t *>(stage + NW * 256 * 8) + w * 256;
+        const int32_t nw = uread(&nlist[0]);
+        for (int64_t q = team_warp(t); q < nw; q += team_nwarps(t)) {
+            const int32_t b = wlist[q], s = bstart[b], m = bstart[b + 1] - s;
+            int P = 32;
+            while (P < m) P <<= 1;
+            for (int x = lane_id(); x < m; x += 32) {
+                wk[x] = keys_out[s + x];
+                wi[x] = idx_out[s + x];
+            }
+            __syncwarp();
+            smem_bitonic(wk, wi, m, P, lane_id(), 32, [] { __syncwarp(); });
+            for (int x = lane_id(); x < m; x += 32) {
+                keys_out[s + x] = wk[x];
+                idx_out[s + x] = wi[x];
+            }
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    // 257..BUCKET_MAX items: a CTA
+    {
+        const int NW = blockDim.x >> 5;
+        char *stage = sm + NW * 1024;
+        uint64_t *ck = reinterpret_cast<uint64_t *>(stage);
+        int32_t *ci = reinterpret_cast<int32_t *>(stage + BUCKET_MAX * 8);
+        const int32_t nc = uread(&nlist[1]);
+        for (int64_t q = t.block(); q < nc; q += t.nblocks()) {
+            const int32_t b = clist[q], s = bstart[b], m = bstart[b + 1] - s;
+            int P = 512;
+            while (P < m) P <<= 1;
+            for (int x = threadIdx.x; x < m; x += blockDim.x) {
+                ck[x] = keys_out[s + x];
+                ci[x] = idx_out[s + x];
+            }
+            __syncthreads();
+            smem_bitonic(ck, ci, m, P, threadIdx.x, blockDim.x, [] { __syncthreads(); });
+            for (int x = threadIdx.x; x < m; x += blockDim.x) {
+                keys_out[s + x] = ck[x];
+                idx_out[s + x] = ci[x];
+            }
+            __syncthreads();
+        }
+    }
+    t.sync();
+    sc.arena.release(am);
+    return true;
+}
+
+// ---------------------------------------------------------------------------
 // off[v] = first k with ids(k) >= v, v in [0, nv]; ids sorted ascending
 // ---------------------------------------------------------------------------
 template <class Team, class Ids>
