@@ -128,9 +128,22 @@ __device__ bool mp_build(const Team &t, Scratch &sc, char *sm, const Graph &A, T
     mp.cost = sc.arena.take<float>(E + 1);
     if (!sc.arena.ok()) return false;
     const uint64_t mask = (nb == 0) ? 0 : ((uint64_t(1) << nb) - 1);
+    // row offsets of the chords: an edge counts the chords before it among
+    // those of its own row
+    // (counted per row and scanned: chords leave long runs of empty rows)
+    int32_t *coff = sc.arena.take<int32_t>((int64_t)nmax + 2);
+    if (!sc.arena.ok()) return false;
+    for (int64_t v = t.rank(); v <= nmax; v += t.size()) coff[v] = 0;
+    t.sync();
+    for (int64_t k = t.rank(); k < nu_n; k += t.size()) atomicAdd(&coff[(int32_t)(nu[k] >> nb)], 1);
+    t.sync();
+    team_scan<Team, int64_t>(
+        t, sc, sm, (int64_t)nmax + 1, [&](int64_t v) -> int64_t { return coff[v]; },
+        [&](int64_t v, int64_t pre, int64_t) { coff[v] = (int32_t)pre; });
     for (int64_t e = t.rank(); e < A.n; e += t.size()) {
-        uint64_t key = pack_key(A.row[e], A.col[e], nb);
-        int64_t lo = 0, hi = nu_n;  // chords < key
+        const int32_t r = A.row[e];
+        uint64_t key = pack_key(r, A.col[e], nb);
+        int64_t lo = coff[r], hi = coff[r + 1];  // chords < key: all of rows < r, then within row r
         while (lo < hi) {
             int64_t m = (lo + hi) >> 1;
             if (nu[m] < key)
