@@ -155,9 +155,20 @@ __device__ void expansion_stage(const Team &t, Scratch &sc, char *sm, TriBuf &tb
     for (int64_t x0 = 0; x0 < X && tb.count <= tb.budget; x0 += CH) {
         const int64_t xn = (X - x0) < CH ? (X - x0) : CH;
         // count
-        for (int64_t q = t.rank(); q < xn; q += t.size()) {
+        // a warp takes 32 consecutive expansions: one search for the owner of
+        // the first, then each lane steps forward to its own
+        for (int64_t qb = (int64_t)team_warp(t) * 32; qb < xn; qb += (int64_t)team_nwarps(t) * 32) {
+            int64_t r0 = lane_id() == 0 ? expansion_owner(xo, R, x0 + qb) : 0;
+            r0 = __shfl_sync(FULL, r0, 0);
+            const int64_t q = qb + lane_id();
+            if (q >= xn) continue;
             const int64_t x = x0 + q;
-            const int64_t r = expansion_owner(xo, R, x);
+            int64_t r = xo ? r0 : x;
+            if (xo) {
+                int steps = 0;  // long runs of rep edges without expansions: search instead
+                while (r < R && xo[r + 1] <= x && ++steps <= 64) ++r;
+                if (steps > 64) r = expansion_owner(xo, R, x);
+            }
             ccount[q] = cnt(r, xo ? x - xo[r] : 0);
         }
         t.sync();
@@ -165,10 +176,20 @@ __device__ void expansion_stage(const Team &t, Scratch &sc, char *sm, TriBuf &tb
             t, sc, sm, xn, [&](int64_t q) -> int64_t { return ccount[q]; },
             [&](int64_t q, int64_t pre, int64_t) { cbase[q] = pre; });
         const int64_t start = tb.count;
-        for (int64_t q = t.rank(); q < xn; q += t.size()) {
-            if (ccount[q] == 0 || start + cbase[q] >= tb.budget) continue;
+        for (int64_t qb = (int64_t)team_warp(t) * 32; qb < xn; qb += (int64_t)team_nwarps(t) * 32) {
+            const int64_t q = qb + lane_id();
+            const bool work = q < xn && ccount[q] != 0 && start + cbase[q] < tb.budget;
+            if (!__any_sync(FULL, work)) continue;
+            int64_t r0 = lane_id() == 0 ? expansion_owner(xo, R, x0 + qb) : 0;
+            r0 = __shfl_sync(FULL, r0, 0);
+            if (!work) continue;
             const int64_t x = x0 + q;
-            const int64_t r = expansion_owner(xo, R, x);
+            int64_t r = xo ? r0 : x;
+            if (xo) {
+                int steps = 0;  // long runs of rep edges without expansions: search instead
+                while (r < R && xo[r + 1] <= x && ++steps <= 64) ++r;
+                if (steps > 64) r = expansion_owner(xo, R, x);
+            }
             emit(r, xo ? x - xo[r] : 0, start + cbase[q]);
         }
         t.sync();

@@ -330,7 +330,7 @@ __device__ __forceinline__ csum_t cs_warp_tree(csum_t a)
     return a;
 }
 
-// returns the sum on every thread; three team syncs
+// returns the sum on every thread; two team syncs
 template <class Team, class Get>
 __device__ double team_csum(const Team &t, Scratch &sc, int64_t n, Get get)
 {
@@ -361,7 +361,9 @@ __device__ double team_csum(const Team &t, Scratch &sc, int64_t n, Get get)
     t.sync();
     double r = uread(&res[0]);
     sc.arena.release(m);
-    t.sync();  // `res` may be reused by the next primitive only after everyone read it
+    // `res` lies in one of the two partial buffers: the next primitive uses the
+    // other one, and the one after it can write this one only after a team
+    // sync that every thread reaches after this read
     return r;
 }
 
