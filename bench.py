@@ -56,6 +56,19 @@ def peaks():
     return 6650.0, "fallback"
 
 
+# DRAM traffic of one k_solve_grid launch (dram__bytes_read.sum +
+# dram__bytes_write.sum), per input edge, from one ncu capture of the
+# profiling-size C2 case (3-D grid 64x64x32 + long range, 753,664 edges, PD):
+# 344,752,640 B read + 1,458,030,592 B written.  The full C2 instance is too
+# large to capture under replay; algorithmic bytes per edge are the same for
+# both sizes (1097 vs 1096 B/edge), so the traffic is scaled by edge count.
+# Command: ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
+#   --clock-control none -k regex:k_solve_grid -s 1 -c 1
+#   python bench.py --config c2s --steps 2 --warmup 1 --no-cpu-baseline
+TRAFFIC_B_PER_EDGE = {("c2", "PD"): (344752640 + 1458030592) / 753664,
+                      ("c2s", "PD"): (344752640 + 1458030592) / 753664}
+
+
 def make_instance(cfg):
     from rama_b200 import instances as I
 
@@ -243,6 +256,8 @@ def run_ours(args, rank, world, local):
     alg = algorithmic_bytes(stats, E)
     kms = statistics.median(kernel_ms)
     achieved = alg / (kms / 1e3) / 1e9
+    tpe = TRAFFIC_B_PER_EDGE.get((cfg, mode)) if stats.team == 2 else None
+    traffic = tpe * E if tpe else None
     line = {
         "metric": "edges/s", "value": value, "unit": "edges/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -258,7 +273,8 @@ def run_ours(args, rank, world, local):
                 "d2h_bytes_per_step": 4 * N + 8, "api": "rama_solve_host"},
         "gpu_launches": args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": None, "peak_source": src, "kernel": "k_solve_grid" if stats.team == 2 else "k_solve_cta",
+                     "traffic": traffic, "peak_source": src,
+                     "kernel": "k_solve_grid" if stats.team == 2 else "k_solve_cta",
                      "kernel_ms": kms, "algorithmic_bytes": alg},
         "clocks": clk.summary(),
     }
