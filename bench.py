@@ -251,7 +251,8 @@ def run_ours(args, rank, world, local):
         return None
     value = world * E * args.steps / (ms_max / 1e3)
     # roofline of the dominant kernel (the solve kernel): algorithmic bytes per
-    # launch over the kernel's average device time
+    # launch (tallied on the device, see algorithmic_bytes) over the kernel's
+    # average device time
     hbm, src = peaks()
     alg = algorithmic_bytes(stats, E)
     kms = statistics.median(kernel_ms)

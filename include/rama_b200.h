@@ -85,7 +85,8 @@ typedef struct {
     int64_t edges_after_dual;
     int64_t workspace_peak;  /* bytes */
     double device_ms;        /* kernel time of the solve (CUDA events) */
-    double alg_bytes;        /* algorithmic bytes of the solve */
+    double alg_bytes;        /* algorithmic bytes of the solve: minimum edge, map, arc and triangle
+                                traffic of each phase, tallied on the device; no sort temporaries */
     double phase_ms[10];     /* time per phase: init, cycle search, MP build, MP iterations + bound,
                                 dual commit, matching, forest contraction set, contraction, other, - */
 } rama_stats;
