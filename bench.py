@@ -149,6 +149,17 @@ class Clocks:
                 "samples": len(sm)}
 
 
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def dist_setup(n_gpus):
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -259,6 +270,7 @@ def run_ours(args, rank, world, local):
     achieved = alg / (kms / 1e3) / 1e9
     tpe = TRAFFIC_B_PER_EDGE.get((cfg, mode)) if stats.team == 2 else None
     traffic = tpe * E if tpe else None
+    phases = phase_roofline(stats, hbm)
     line = {
         "metric": "edges/s", "value": value, "unit": "edges/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
@@ -274,14 +286,31 @@ def run_ours(args, rank, world, local):
                 "d2h_bytes_per_step": 4 * N + 8, "api": "rama_solve_host"},
         "gpu_launches": args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": traffic, "peak_source": src,
-                     "kernel": "k_solve_grid" if stats.team == 2 else "k_solve_cta",
-                     "kernel_ms": kms, "algorithmic_bytes": alg},
+                     "traffic": traffic, "peak_source": src, "kernel": KERNEL_OF_TEAM.get(stats.team, "?"),
+                     "kernel_ms": kms, "algorithmic_bytes": alg, "phases": phases},
         "clocks": clk.summary(),
     }
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, mode)
     return line
+
+
+KERNEL_OF_TEAM = {1: "k_solve_cta", 2: "k_solve_grid", 3: "k_solve_mixed"}
+
+
+def phase_roofline(stats, hbm):
+    """Per phase of the last solve: device time, algorithmic bytes (tallied
+    on the device), achieved GB/s and the fraction of the HBM peak."""
+    from rama_b200 import _lib
+
+    out = {}
+    for k, name in enumerate(_lib.PHASES):
+        ms, b = float(stats.phase_ms[k]), float(stats.phase_bytes[k])
+        if name == "-" or (ms == 0.0 and b == 0.0):
+            continue
+        gbs = b / (ms / 1e3) / 1e9 if ms > 0 else 0.0
+        out[name] = {"ms": round(ms, 3), "bytes": b, "gbs": round(gbs, 1), "frac": round(gbs / hbm, 4)}
+    return out
 
 
 def algorithmic_bytes(stats, E):
@@ -475,13 +504,18 @@ def cpu_baseline(cfg, mode):
     for (ii, jj, cc) in insts:
         glab = O.gaec(ii, jj, cc)
     t3 = time.perf_counter()
+    edges = sum(len(x[2]) for x in insts)
     i, j, c = insts[-1]
-    return {"value": len(c) / (t1 - t0), "unit": "edges/s", "cores": 1, "kind": "port",
-            "sample": f"{desc}: {len(c)} edges, mode {mode}, oracle restatement of the RAMA solve, "
+    gaec_obj = O.objective(i, j, c, glab)
+    rama_obj = O.objective(i, j, c, lab)
+    return {"value": edges / (t1 - t0), "unit": "edges/s", "cores": 1, "kind": "port",
+            "sample": f"{desc}: {edges} edges, mode {mode}, oracle restatement of the RAMA solve, "
                       f"{t1 - t0:.2f} s",
-            "gaec": {"value": len(c) / (t3 - t2), "unit": "edges/s", "cores": 1,
-                     "objective": O.objective(i, j, c, glab), "rama_oracle_objective": O.objective(i, j, c, lab)},
-            "host_cores": os.cpu_count()}
+            "gaec_value": edges / (t3 - t2), "gaec_objective": gaec_obj, "rama_oracle_objective": rama_obj,
+            "gaec": {"value": edges / (t3 - t2), "unit": "edges/s", "cores": 1,
+                     "what": "project-written sequential greedy additive edge contraction + union-find",
+                     "objective": gaec_obj, "rama_oracle_objective": rama_obj},
+            "cpu_model": cpu_model(), "host_cores": os.cpu_count()}
 
 
 def run_reference_many(args, local, R):
@@ -526,6 +560,15 @@ def run_reference_many(args, local, R):
     tot_s = sum(times) / 1e3
     value = edges / tot_s
     lat = np.asarray(times)
+    # end to end through the reference's host overload (host arrays in, labels
+    # out: 12 B per edge in, 4 B per node out)
+    e2e_s, h2d, d2h = 0.0, 0, 0
+    for (i, j, c), mode in sample:
+        t0 = time.perf_counter()
+        lab_h, _, _ = R.rama(i, j, c, mode)
+        e2e_s += time.perf_counter() - t0
+        h2d += 12 * len(c)
+        d2h += 4 * len(lab_h)
     return {
         "impl": "reference", "metric": "edges/s", "value": value, "unit": "edges/s", "n_gpus": 1,
         "steps": len(times), "warmup": args.warmup, "ms_per_step": float(lat.mean()), "higher_is_better": True,
@@ -533,7 +576,9 @@ def run_reference_many(args, local, R):
         "config": {"workload": CONFIGS[cfg]["desc"], "sample": what, "edges": edges},
         "solves_per_s": len(times) / tot_s, "p50_ms": float(np.percentile(lat, 50)),
         "p99_ms": float(np.percentile(lat, 99)),
-        "e2e": {"value": value, "unit": "edges/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "e2e": {"value": edges / e2e_s, "unit": "edges/s", "h2d_bytes_per_step": h2d // max(1, len(times)),
+                "d2h_bytes_per_step": d2h // max(1, len(times)),
+                "api": "rama_cuda(const std::vector<int>&, ...) host overload, one call per instance"},
         "cpu_baseline": {"value": value, "unit": "edges/s", "cores": 0, "kind": "reference",
                          "sample": what + " (the reference solver built from source for sm_100a; it has no CPU "
                                           "path)"},
@@ -598,8 +643,8 @@ def run_reference(args, rank, world, local):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": CONFIGS[cfg]["desc"], "edges": E, "nodes": N, "mode": mode},
         "objective": obj, "lower_bound": lbv,
-        "e2e": {"value": E / statistics.median(e2e), "unit": "edges/s", "h2d_bytes_per_step": 0,
-                "d2h_bytes_per_step": 0},
+        "e2e": {"value": E / statistics.median(e2e), "unit": "edges/s", "h2d_bytes_per_step": 12 * E,
+                "d2h_bytes_per_step": 4 * N, "api": "rama_cuda(const std::vector<int>&, ...) host overload"},
         "cpu_baseline": {"value": value, "unit": "edges/s", "cores": 0, "kind": "reference",
                          "sample": "the reference solver itself (built from source for sm_100a into oracle/_ref) "
                                    "on the full workload; it runs on the GPU -- the reference has no CPU path"},
@@ -639,7 +684,6 @@ def main():
 
         dist.destroy_process_group()
     sys.stdout.flush()
-    os._exit(0)
 
 
 if __name__ == "__main__":

@@ -89,6 +89,7 @@ typedef struct {
                                 traffic of each phase, tallied on the device; no sort temporaries */
     double phase_ms[10];     /* time per phase: init, cycle search, MP build, MP iterations + bound,
                                 dual commit, matching, forest contraction set, contraction, other, - */
+    double phase_bytes[10];  /* algorithmic bytes per phase (same order), the parts of alg_bytes */
 } rama_stats;
 
 /*
@@ -159,11 +160,20 @@ int rama_batch_wait(rama_handle h, int64_t *num_labels, double *lbs, int32_t *st
  * at most RAMA_STATIC_MAX_EDGES edges and node ids below
  * RAMA_STATIC_MAX_NODES; larger instances are rejected with
  * RAMA_ERR_INVALID_ARG, and an instance whose solve needs more scratch than
- * the array returns RAMA_ERR_OOM.  dump_timeline is ignored.
- * The first call on a device looks up the array's device address and sets the
- * kernel's shared-memory limit; make that first call before any stream capture.  All calls share the one array: calls
- * that overlap on the GPU (other streams or host threads) race and must be
- * serialised by the caller.
+ * the array returns RAMA_ERR_OOM.  As in rama_solve, a dual that runs out of
+ * scratch falls back to the trivial bound and the call still succeeds.
+ * dump_timeline is ignored.  The call is synchronous: it returns once the
+ * solve on `stream` has finished.
+ * The array is device memory of the library's module: CUDA reserves it on a
+ * device when the module loads there, which with lazy module loading (the
+ * default) is the first call into the library on that device.  A caller whose
+ * pool allocator claims the device's memory should make one call (for example
+ * an empty instance) before the pool reserves its memory.
+ * The first call on a device also looks up the array's device address and
+ * sets the kernel's shared-memory limit; make that first call before any
+ * stream capture.  All calls share the one array: calls that overlap on the
+ * GPU (other streams or host threads) race and must be serialised by the
+ * caller.
  */
 #define RAMA_STATIC_MAX_EDGES 30000
 #define RAMA_STATIC_MAX_NODES 65536

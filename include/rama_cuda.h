@@ -4,6 +4,7 @@
 // the reference's message "Found bad contractions"); an exhausted workspace
 // throws std::bad_alloc.
 #pragma once
+#include <algorithm>
 #include <memory>
 #include <new>
 #include <stdexcept>
@@ -77,6 +78,7 @@ inline std::tuple<std::vector<int>, double, int, std::vector<std::vector<int>>> 
 
 #if defined(__CUDACC__) || defined(RAMA_WITH_THRUST)
 #include <thrust/device_vector.h>
+#include <thrust/extrema.h>
 // Device overload: consumes the inputs, returns (labels, lower bound, timeline).
 inline std::tuple<thrust::device_vector<int>, double, std::vector<std::vector<int>>> rama_cuda(
     thrust::device_vector<int> &&i, thrust::device_vector<int> &&j, thrust::device_vector<float> &&costs,

@@ -2,11 +2,19 @@
 # Builds the reference solver (pawelswoboda/RAMA) from its sources, where they
 # lie, together with oracle/ref_harness.cu into oracle/_ref/librama_ref.so.
 # Test infrastructure: the result is the parity oracle on the GPU and the
-# reference arm of bench.py.  Needs the reference tree (default
-# /root/reference); nothing from it is copied into this repository.
+# reference arm of bench.py.  Nothing from the reference is copied into this
+# repository.
+#
+#   oracle/build_ref.sh <reference tree>     (or RAMA_REFERENCE_DIR=<tree>)
+#
+# Without a reference tree the prebuilt oracle/_ref is kept.
 set -euo pipefail
 HERE="$(cd "$(dirname "${BASH_SOURCE[0]}")" && pwd)"
-REF="${RAMA_REFERENCE_DIR:-/root/reference}"
+REF="${1:-${RAMA_REFERENCE_DIR:-}}"
+if [ -z "$REF" ]; then
+  echo "usage: $0 <reference tree> (or set RAMA_REFERENCE_DIR); keeping the prebuilt oracle/_ref" >&2
+  exit 0
+fi
 OUT="$HERE/_ref"
 OBJ="$OUT/obj"
 if [ ! -d "$REF/src" ]; then

@@ -57,6 +57,7 @@ class RamaStats(C.Structure):
         ("device_ms", C.c_double),
         ("alg_bytes", C.c_double),
         ("phase_ms", C.c_double * 10),
+        ("phase_bytes", C.c_double * 10),
     ]
 
 PHASES = ("init", "cycles", "mp_build", "mp_iter", "dual_commit", "matching", "woc", "contract", "other", "-")

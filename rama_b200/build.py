@@ -29,9 +29,9 @@ NVCC_FLAGS = [
     "--expt-relaxed-constexpr", "--extended-lambda",
     "-Xcompiler", "-fPIC",
 ]
-# RAMA_SPLIT_COMPILE=1 optimises and assembles the kernels of one unit on all
-# host cores (capi.cu: about 5 minutes instead of 14 on 8 cores).  Development
-# builds only: the C2 solve measured about 2 % slower built that way.
+# RAMA_SPLIT_COMPILE=1 also splits the optimisation of each unit over the
+# host cores.  Development builds only: the C2 solve measured about 2 % slower
+# built that way.
 if os.environ.get("RAMA_SPLIT_COMPILE") == "1":
     NVCC_FLAGS.append("--split-compile=0")
 
@@ -44,17 +44,22 @@ def _stale(target, sources):
 
 
 def build_lib(force=False, verbose=False):
-    """Compiles every csrc/*.cu to an object (in parallel) and links the .so."""
-    srcs = glob.glob(os.path.join(HERE, "csrc", "*")) + [os.path.join(INCLUDE, "rama_b200.h")]
-    if not force and not _stale(LIB, srcs):
-        return LIB
-    objdir = os.path.join(HERE, "_build")
-    os.makedirs(objdir, exist_ok=True)
+    """Compiles every stale csrc/*.cu to an object (all in parallel: each
+    kernel has a translation unit of its own) and links the .so.  An object
+    is stale when its .cu, any header or the C ABI header is newer."""
+    headers = glob.glob(os.path.join(HERE, "csrc", "*.cuh")) + [os.path.join(INCLUDE, "rama_b200.h")]
     units = sorted(glob.glob(os.path.join(HERE, "csrc", "*.cu")))
+    objdir = os.path.join(HERE, "_build")
+    objects = [os.path.join(objdir, os.path.basename(u)[:-3] + ".o") for u in units]
+    if not force and not _stale(LIB, units + headers) and all(os.path.exists(o) for o in objects):
+        return LIB
+    os.makedirs(objdir, exist_ok=True)
     procs, objs = [], []
     for u in units:
         o = os.path.join(objdir, os.path.basename(u)[:-3] + ".o")
         objs.append(o)
+        if not force and not _stale(o, [u] + headers):
+            continue
         cmd = [NVCC, *NVCC_FLAGS, "-c", "-o", o, u]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")

@@ -1,12 +1,13 @@
-// capi.cu -- kernels and the C ABI of librama_b200.so (include/rama_b200.h).
+// capi.cu -- the host side of librama_b200.so: the C ABI of
+// include/rama_b200.h (handles, workspaces, launches, batches, statistics).
 //
-// Two kernels run the same device solver (solver.cuh):
-//   k_solve_cta  : persistent CTAs; each pulls instances from a queue (largest
-//                  first) and solves them alone (BlockTeam).  Used for batches
-//                  and for small single instances.
-//   k_solve_grid : one cooperative launch; the whole GPU solves one instance
-//                  (GridTeam).
-// Both take their scratch memory from a workspace the handle owns.
+// The kernels live in their own translation units (kernels.cuh):
+//   k_solve_grid  : one cooperative launch; the whole GPU solves one instance.
+//   k_solve_mixed : clusters of CTAs for the largest instances of a batch (and
+//                   single mid-size solves), then one CTA per instance.
+//   k_solve_cta   : persistent CTAs, one instance each.
+//   k_step_*, k_objective, k_parse_grid, k_max_id: steps and helpers.
+// Every solve takes its scratch memory from a workspace the handle owns.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -18,15 +19,12 @@
 #include <vector>
 
 #include "../../include/rama_b200.h"
-#include "parse.cuh"
-#include "solver.cuh"
+#include "kernels.cuh"
 
 using namespace rama;
 
 namespace {
 
-constexpr int THREADS = 512;
-constexpr int SMEM = sort_smem_bytes(THREADS) + 1024;
 constexpr int CLUSTER_CTAS = 8;               // CTAs of a cluster team (the portable maximum)
 constexpr int64_t CLUSTER_MIN_EDGES = 20000;   // smaller batch instances always run on one CTA
 constexpr int64_t SINGLE_CLUSTER_MIN = 4000;   // a single solve from this size on runs on a cluster
@@ -45,311 +43,6 @@ int fail(int code, const std::string &msg)
         cudaError_t e_ = (call);                                                               \
         if (e_ != cudaSuccess) return fail(RAMA_ERR_CUDA, std::string(#call ": ") + cudaGetErrorString(e_)); \
     } while (0)
-
-__device__ __forceinline__ Scratch make_scratch(char *base, uint64_t bytes) { return scratch_over(base, bytes); }
-
-struct CtaLaunch {
-    Instance *inst;
-    const int32_t *order;
-    int32_t count;
-    int32_t *queue;
-};
-
-__global__ void __launch_bounds__(THREADS, 2) k_solve_cta(CtaLaunch L)
-{
-    extern __shared__ __align__(16) char sm[];
-    __shared__ int next;
-    BlockTeam t;
-    for (int guard = 0; guard < (1 << 30); ++guard) {
-        if (threadIdx.x == 0) next = atomicAdd(L.queue, 1);
-        __syncthreads();
-        const int k = next;
-        __syncthreads();
-        if (k >= L.count) break;
-        Instance *io = &L.inst[L.order[k]];
-        Scratch sc = make_scratch(io->ws, io->ws_bytes);
-        solve_instance(t, sm, sc, io);
-        __syncthreads();
-    }
-}
-
-// A batch with instances for clusters: clusters of CLUSTER_CTAS CTAs draw
-// from the queue, which holds the cluster instances first (largest first);
-// once a cluster draws an instance that is not for a cluster, its CTAs go on
-// alone, one instance each, like k_solve_cta.
-struct MixedLaunch {
-    Instance *inst;
-    const int32_t *order;
-    int32_t count;
-    int32_t ncluster;  // queue entries [0, ncluster) are solved by a cluster
-    int32_t *queue;
-};
-
-__global__ void __launch_bounds__(THREADS, 2) k_solve_mixed(MixedLaunch L)
-{
-    extern __shared__ __align__(16) char sm[];
-    __shared__ int next;
-    cg::cluster_group cl = cg::this_cluster();
-    ClusterTeam ct;
-    BlockTeam bt;
-    int mine = -1;  // an instance this CTA drew for itself
-    for (int guard = 0; guard < (1 << 30); ++guard) {
-        if (cl.block_rank() == 0 && threadIdx.x == 0) next = atomicAdd(L.queue, 1);
-        cl.sync();
-        const int k = *cl.map_shared_rank(&next, 0);
-        cl.sync();  // no CTA reads another's shared memory after this point
-        if (k >= L.count) return;
-        if (k >= L.ncluster) {
-            if (cl.block_rank() == 0) mine = k;
-            break;
-        }
-        Instance *io = &L.inst[L.order[k]];
-        solve_instance(ct, sm, make_scratch(io->ws, io->ws_bytes), io);
-        cl.sync();
-    }
-    for (int guard = 0; guard < (1 << 30); ++guard) {
-        int k = mine;
-        mine = -1;
-        if (k < 0) {
-            if (threadIdx.x == 0) next = atomicAdd(L.queue, 1);
-            __syncthreads();
-            k = next;
-            __syncthreads();
-        }
-        if (k >= L.count) break;
-        Instance *io = &L.inst[L.order[k]];
-        solve_instance(bt, sm, make_scratch(io->ws, io->ws_bytes), io);
-        __syncthreads();
-    }
-}
-
-struct GridLaunch {
-    Instance *inst;
-    char *ws;
-    uint64_t ws_bytes;
-};
-
-// MULTICUT text -> triples on the cooperative grid
-struct ParseLaunch {
-    const char *text;
-    int64_t len;
-    int32_t *i, *j;
-    float *c;
-    int64_t cap;
-    int64_t *out;  // count, -1 bad first line, -2 workspace exhausted
-    char *ws;
-    uint64_t ws_bytes;
-};
-
-__global__ void __launch_bounds__(THREADS, 2) k_parse_grid(ParseLaunch L)
-{
-    extern __shared__ __align__(16) char sm[];
-    GridTeam t;
-    Scratch sc = make_scratch(L.ws, L.ws_bytes);
-    if (t.rank() == 0) *sc.err = 0;
-    t.sync();
-    const int64_t n = parse_multicut(t, sc, sm, L.text, L.len, L.i, L.j, L.c, L.cap);
-    if (t.leader()) L.out[0] = sc.arena.ok() ? n : -2;
-}
-
-__global__ void __launch_bounds__(THREADS, 2) k_solve_grid(GridLaunch L)
-{
-    extern __shared__ __align__(16) char sm[];
-    GridTeam t;
-    Scratch sc = make_scratch(L.ws, L.ws_bytes);
-    solve_instance(t, sm, sc, L.inst);
-}
-
-// ---------------------------------------------------------------------------
-// single steps
-// ---------------------------------------------------------------------------
-template <class Team>
-__device__ void copy_graph_out(const Team &t, const Graph &g, rama_step_args *a)
-{
-    if (g.n <= a->out_cap)
-        for (int64_t e = t.rank(); e < g.n; e += t.size()) {
-            a->out_row[e] = g.row[e];
-            a->out_col[e] = g.col[e];
-            a->out_cost[e] = g.cost[e];
-        }
-    if (t.leader()) {
-        a->out_n = g.n;
-        a->out_rows = g.rows;
-        a->out_cols = g.cols;
-        if (g.n > a->out_cap) a->status |= ERR_INVALID_ARG;
-    }
-}
-
-template <class Team>
-__device__ void run_step(const Team &t, char *sm, Scratch sc, rama_step_args *a)
-{
-    if (t.rank() == 0) *sc.err = 0;
-    t.sync();
-    Graph A;
-    A.row = const_cast<int32_t *>(a->row);
-    A.col = const_cast<int32_t *>(a->col);
-    A.cost = const_cast<float *>(a->cost);
-    A.n = a->n;
-    A.rows = a->rows;
-    A.cols = a->cols;
-    const int op = a->op;
-    if (op == RAMA_STEP_INIT) {
-        Graph g = graph_from_edges(t, sc, sm, a->i, a->j, a->c, a->m);
-        if (sc.arena.ok()) copy_graph_out(t, g, a);
-    } else if (op == RAMA_STEP_CONTRACT) {
-        int32_t mx = team_max<Team, int32_t>(t, sc, sm, a->map_size, 0, [&](int64_t k) { return a->map[k]; });
-        Graph g = graph_contract_raw(t, sc, sm, A, a->map, mx);
-        if (sc.arena.ok()) copy_graph_out(t, g, a);
-    } else if (op == RAMA_STEP_MATCHING) {
-        int32_t M = 0;
-        int32_t nr = matching_contraction_map(t, sc, sm, A, a->mean_multiplier_mm, a->out_map, &M);
-        if (t.leader()) {
-            a->out_nr = nr;
-            a->out_count = M;
-        }
-    } else if (op == RAMA_STEP_WOC) {
-        int32_t sz = 0;
-        int err = 0;
-        int32_t nr = woc_contraction_map(t, sc, sm, A, a->out_map, &sz, &err, a->max_cycle_length >= 5);
-        if (t.leader()) {
-            a->out_nr = nr;
-            a->out_count = sz;
-            a->status |= err;
-        }
-    } else if (op == RAMA_STEP_MSF) {
-        int32_t mx = team_max<Team, int32_t>(t, sc, sm, a->m, 0, [&](int64_t e) { return max(a->i[e], a->j[e]); });
-        bool ok = team_msf(t, sc, sm, a->m, mx + 1, [&](int64_t e) { return a->i[e]; },
-                           [&](int64_t e) { return a->j[e]; }, [&](int64_t e) { return a->c[e]; }, a->out_flags);
-        if (t.leader() && !ok) a->status |= ERR_ITER_LIMIT;
-    } else if (op == RAMA_STEP_CC) {
-        const int32_t *off = a->offsets;
-        const int32_t nn = a->num_nodes;
-        bool ok = team_cc(
-            t, sc, nn, a->adj_len,
-            [&](int64_t k) {
-                int32_t lo = 0, hi = nn - 1;  // row of entry k: last v with off[v] <= k
-                while (lo < hi) {
-                    int32_t mid = (lo + hi + 1) >> 1;
-                    if (off[mid] <= k)
-                        lo = mid;
-                    else
-                        hi = mid - 1;
-                }
-                return lo;
-            },
-            [&](int64_t k) { return a->adj[k]; }, a->out_map);
-        if (t.leader() && !ok) a->status |= ERR_ITER_LIMIT;
-    } else if (op == RAMA_STEP_CYCLES) {
-        TriBuf tb;
-        conflicted_cycles(t, sc, sm, A, a->max_cycle_length, a->tri_memory_factor, a->tol, tb);
-        if (sc.arena.ok()) {
-            if (tb.num <= a->out_tri_cap)
-                for (int64_t k = t.rank(); k < tb.num; k += t.size()) {
-                    a->out_t1[k] = tb.t1[k];
-                    a->out_t2[k] = tb.t2[k];
-                    a->out_t3[k] = tb.t3[k];
-                }
-            if (t.leader()) {
-                a->out_count = tb.num;
-                a->out_raw = tb.count;
-                if (tb.num > a->out_tri_cap) a->status |= ERR_INVALID_ARG;
-            }
-        }
-    } else if (op == RAMA_STEP_MP) {
-        TriBuf tb;
-        tb.budget = a->T;
-        tb.count = a->T;
-        tb.num = a->T;
-        tb.t1 = sc.arena.take<int32_t>(a->T + 1);
-        tb.t2 = sc.arena.take<int32_t>(a->T + 1);
-        tb.t3 = sc.arena.take<int32_t>(a->T + 1);
-        if (sc.arena.ok()) {
-            for (int64_t k = t.rank(); k < a->T; k += t.size()) {
-                tb.t1[k] = a->t1[k];
-                tb.t2[k] = a->t2[k];
-                tb.t3[k] = a->t3[k];
-            }
-            t.sync();
-            Mp mp;
-            if (mp_build(t, sc, sm, A, tb, mp)) {
-                double lb0 = mp_lower_bound(t, sc, mp);
-                for (int it = 0; it < a->num_iter; ++it) mp_iteration(t, mp);
-                double lb1 = mp_lower_bound(t, sc, mp);
-                Graph g;
-                g.row = mp.row;
-                g.col = mp.col;
-                g.cost = mp.cost;
-                g.n = mp.E;
-                graph_set_dims(t, sc, sm, g);
-                copy_graph_out(t, g, a);
-                if (t.leader()) {
-                    a->out_lb0 = lb0;
-                    a->out_lb1 = lb1;
-                    a->out_count = mp.T;
-                }
-            }
-        }
-    } else if (op == RAMA_STEP_DUAL) {
-        int64_t nt = 0;
-        int oom = 0;
-        double lb = dual_solver(t, sc, sm, A, a->max_cycle_length, a->num_iter, a->tri_memory_factor, a->num_outer,
-                                a->tol, &nt, &oom);
-        copy_graph_out(t, A, a);
-        if (t.leader()) {
-            a->out_lb0 = lb;
-            a->out_raw = nt;
-            a->out_nr = oom;
-        }
-    } else if (op == RAMA_STEP_CSUM) {
-        double s = team_csum(t, sc, a->m, [&](int64_t k) -> double { return (double)a->c[k]; });
-        if (t.leader()) a->out_lb0 = s;
-    } else if (op == RAMA_STEP_SORT) {
-        uint64_t *k1 = sc.arena.take<uint64_t>(a->m + 1), *k2 = sc.arena.take<uint64_t>(a->m + 1);
-        int32_t *v1 = sc.arena.take<int32_t>(a->m + 1), *v2 = sc.arena.take<int32_t>(a->m + 1);
-        if (sc.arena.ok()) {
-            for (int64_t k = t.rank(); k < a->m; k += t.size()) {
-                k1[k] = a->keys[k];
-                v1[k] = a->i[k];
-            }
-            t.sync();
-            team_sort_pairs(t, sc, sm, k1, v1, k2, v2, a->m, a->key_bits);
-            for (int64_t k = t.rank(); k < a->m; k += t.size()) {
-                a->out_keys[k] = k1[k];
-                a->out_map[k] = v1[k];
-            }
-        }
-    }
-    t.sync();
-    if (t.leader()) {
-        if (!sc.arena.ok()) a->status |= ERR_ARENA;
-        if (__ldcg(sc.err)) a->status |= ERR_ITER_LIMIT;
-    }
-}
-
-__global__ void __launch_bounds__(THREADS, 2) k_step_cta(rama_step_args *a, char *ws, uint64_t bytes)
-{
-    extern __shared__ __align__(16) char sm[];
-    BlockTeam t;
-    run_step(t, sm, make_scratch(ws, bytes), a);
-}
-
-__global__ void __launch_bounds__(THREADS, 2) k_step_grid(rama_step_args *a, char *ws, uint64_t bytes)
-{
-    extern __shared__ __align__(16) char sm[];
-    GridTeam t;
-    run_step(t, sm, make_scratch(ws, bytes), a);
-}
-
-// objective: CSUM over edges whose endpoints carry different labels
-__global__ void __launch_bounds__(THREADS, 2) k_objective(const int32_t *I, const int32_t *J, const float *C, int64_t n,
-                                                          const int32_t *lab, double *out, char *ws, uint64_t bytes)
-{
-    extern __shared__ __align__(16) char sm[];
-    GridTeam t;
-    Scratch sc = make_scratch(ws, bytes);
-    double s = team_csum(t, sc, n, [&](int64_t e) -> double { return lab[I[e]] != lab[J[e]] ? (double)C[e] : 0.0; });
-    if (t.leader()) *out = s;
-}
 
 int status_from_bits(int32_t s)
 {
@@ -417,6 +110,7 @@ struct rama_context {
     // device staging of rama_solve_host (grown on demand, reused)
     int32_t *io_i = nullptr, *io_j = nullptr, *io_l = nullptr;
     float *io_c = nullptr;
+    cudaStream_t io_stream = nullptr;  // rama_solve_host's copies and solve
     int64_t io_edges = 0, io_labels = 0;
     // asynchronous batch in flight
     bool b_active = false;
@@ -515,6 +209,7 @@ int solve_one(rama_context *h, const int32_t *d_i, const int32_t *d_j, const flo
               cudaStream_t st)
 {
     if (!h || !opts || n < 0 || (n > 0 && (!d_i || !d_j || !d_c))) return fail(RAMA_ERR_INVALID_ARG, "bad arguments");
+    if (h->b_active) return fail(RAMA_ERR_INVALID_ARG, "a batch is in flight on this handle (call rama_batch_wait)");
     Options o = to_opts(opts);
     int team = opts->team;
     if (team < 1 || team > 3) team = n < SINGLE_CLUSTER_MIN ? 1 : (n < GRID_MIN_EDGES ? 3 : 2);
@@ -549,7 +244,7 @@ int solve_one(rama_context *h, const int32_t *d_i, const int32_t *d_j, const flo
         hi.prof = h->d_prof;
         hi.ws = h->ws;
         hi.ws_bytes = h->ws_bytes;
-        CU(cudaMemsetAsync(h->d_prof, 0, sizeof(int64_t) * PH_COUNT, st));
+        CU(cudaMemsetAsync(h->d_prof, 0, sizeof(int64_t) * 2 * PH_COUNT, st));
         int32_t zero = 0;
         CU(cudaMemcpyAsync(h->d_inst, &hi, sizeof(Instance), cudaMemcpyHostToDevice, st));
         CU(cudaMemcpyAsync(h->d_order, &zero, sizeof(int32_t), cudaMemcpyHostToDevice, st));
@@ -582,9 +277,12 @@ int solve_one(rama_context *h, const int32_t *d_i, const int32_t *d_j, const flo
         h->stats.device_ms = ms;
         h->stats.alg_bytes = ho.alg_bytes;
         {
-            int64_t pr[PH_COUNT];
+            int64_t pr[2 * PH_COUNT];
             CU(cudaMemcpy(pr, h->d_prof, sizeof(pr), cudaMemcpyDeviceToHost));
-            for (int k = 0; k < PH_COUNT && k < 10; ++k) h->stats.phase_ms[k] = 1e-6 * (double)pr[k];
+            for (int k = 0; k < PH_COUNT && k < 10; ++k) {
+                h->stats.phase_ms[k] = 1e-6 * (double)pr[k];
+                h->stats.phase_bytes[k] = (double)pr[PH_COUNT + k];
+            }
         }
         if (opts->dump_timeline && ho.timeline_rounds > 0) {
             h->tl_rounds = ho.timeline_rounds;
@@ -705,7 +403,7 @@ int rama_create(int device, uint64_t workspace_bytes, rama_handle *out)
     CU(cudaMalloc(&h->d_queue, sizeof(int32_t) * 4));
     CU(cudaMalloc(&h->d_step, sizeof(rama_step_args)));
     CU(cudaMalloc(&h->d_scalar, sizeof(double) * 4));
-    CU(cudaMalloc(&h->d_prof, sizeof(int64_t) * PH_COUNT));
+    CU(cudaMalloc(&h->d_prof, sizeof(int64_t) * 2 * PH_COUNT));
     CU(cudaEventCreate(&h->ev0));
     CU(cudaEventCreate(&h->ev1));
     CU(cudaEventCreateWithFlags(&h->ev_done, cudaEventDisableTiming));
@@ -733,6 +431,7 @@ void rama_destroy(rama_handle h)
     cudaEventDestroy(h->ev0);
     cudaEventDestroy(h->ev1);
     cudaEventDestroy(h->ev_done);
+    if (h->io_stream) cudaStreamDestroy(h->io_stream);
     if (h->b_host) cudaFreeHost(h->b_host);
     delete h;
 }
@@ -753,9 +452,8 @@ int rama_solve_host(rama_handle h, const int32_t *i, const int32_t *j, const flo
 {
     if (!h || !opts || n < 0 || (n > 0 && (!i || !j || !costs))) return fail(RAMA_ERR_INVALID_ARG, "bad arguments");
     CU(cudaSetDevice(h->device));
-    int32_t mx = -1;
-    for (int64_t e = 0; e < n; ++e) mx = std::max(mx, std::max(i[e], j[e]));
-    const int64_t cap = (int64_t)mx + 1;
+    if (!h->io_stream) CU(cudaStreamCreateWithFlags(&h->io_stream, cudaStreamNonBlocking));
+    cudaStream_t st = h->io_stream;
     if (h->io_edges < std::max<int64_t>(n, 1)) {
         cudaFree(h->io_i);
         cudaFree(h->io_j);
@@ -769,6 +467,28 @@ int rama_solve_host(rama_handle h, const int32_t *i, const int32_t *j, const flo
         CU(cudaMalloc(&h->io_c, nb));
         h->io_edges = std::max<int64_t>(n, 1);
     }
+    int32_t *di = h->io_i, *dj = h->io_j;
+    float *dc = h->io_c;
+    if (n > 0) {
+        CU(cudaMemcpyAsync(di, i, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(dj, j, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
+        CU(cudaMemcpyAsync(dc, costs, sizeof(float) * n, cudaMemcpyHostToDevice, st));
+    }
+    // the label buffer holds max node id + 1 entries: the maximum comes from
+    // the device copy of the edges, not from a scan on the host
+    int32_t mx[2] = {-1, 0};
+    int32_t *d_mx = reinterpret_cast<int32_t *>(h->d_scalar);
+    CU(cudaMemcpyAsync(d_mx, mx, sizeof(mx), cudaMemcpyHostToDevice, st));
+    if (n > 0) {
+        const int64_t want = (n / 4 + 255) / 256;
+        const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)h->sms * 8));
+        k_max_id<<<blocks, 256, 0, st>>>(MaxIdLaunch{di, dj, n, d_mx});
+        CU(cudaGetLastError());
+    }
+    CU(cudaMemcpyAsync(mx, d_mx, sizeof(mx), cudaMemcpyDeviceToHost, st));
+    CU(cudaStreamSynchronize(st));
+    if (mx[1]) return fail(RAMA_ERR_INVALID_ARG, "invalid input (negative node id)");
+    const int64_t cap = (int64_t)mx[0] + 1;
     if (h->io_labels < std::max<int64_t>(cap, 1)) {
         cudaFree(h->io_l);
         h->io_l = nullptr;
@@ -776,19 +496,17 @@ int rama_solve_host(rama_handle h, const int32_t *i, const int32_t *j, const flo
         CU(cudaMalloc(&h->io_l, sizeof(int32_t) * (size_t)std::max<int64_t>(cap, 1)));
         h->io_labels = std::max<int64_t>(cap, 1);
     }
-    int32_t *di = h->io_i, *dj = h->io_j, *dl = h->io_l;
-    float *dc = h->io_c;
-    cudaStream_t st = nullptr;
-    CU(cudaMemcpyAsync(di, i, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
-    CU(cudaMemcpyAsync(dj, j, sizeof(int32_t) * n, cudaMemcpyHostToDevice, st));
-    CU(cudaMemcpyAsync(dc, costs, sizeof(float) * n, cudaMemcpyHostToDevice, st));
+    int32_t *dl = h->io_l;
     int64_t nl = 0;
     int rc = solve_one(h, di, dj, dc, n, opts, dl, cap, &nl, lb, st);
     if (rc == RAMA_OK) {
         if (nl > labels_cap)
             rc = fail(RAMA_ERR_INVALID_ARG, "label buffer too small");
-        else if (nl > 0 && cudaMemcpy(labels, dl, sizeof(int32_t) * nl, cudaMemcpyDeviceToHost) != cudaSuccess)
-            rc = fail(RAMA_ERR_CUDA, "copying labels failed");
+        else if (nl > 0) {
+            if (cudaMemcpyAsync(labels, dl, sizeof(int32_t) * nl, cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+                cudaStreamSynchronize(st) != cudaSuccess)
+                rc = fail(RAMA_ERR_CUDA, "copying labels failed");
+        }
         if (num_labels) *num_labels = nl;
         if (solve_ms) *solve_ms = h->stats.device_ms;
     }

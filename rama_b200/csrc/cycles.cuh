@@ -214,14 +214,41 @@ __device__ void conflicted_cycles(const Team &t, Scratch &sc, char *sm, const Gr
     const float thresh = mn * tol;          // determine_threshold (:170-174)
     const float pos_tol = -1.0f * thresh;   // create_matrices (:176-220)
     const int32_t N = A.max_dim();
+    // Every conflicted cycle closes a repulsive edge (u, v) with a path of
+    // attractive edges, so both u and v have an attractive edge.  Repulsive
+    // edges without one at either end emit nothing: they are left out of the
+    // search (the emission order of the others, and so the budget's
+    // truncation, is unchanged), and a graph with none left needs no CSR.
     int64_t *ridx = sc.arena.take<int64_t>(A.n + 1);
+    int8_t *haspos = sc.arena.take<int8_t>((int64_t)N + 1);
     if (!sc.arena.ok()) return;
-    const int64_t R = team_compact(
-        t, sc, sm, A.n, [&](int64_t e) { return A.cost[e] < thresh; }, [&](int64_t e, int64_t p) { ridx[p] = e; });
-    const int64_t P = team_sum<Team, int64_t>(t, sc, sm, A.n, [&](int64_t e) -> int64_t { return A.cost[e] > pos_tol; });
-    if (P == 0 || R == 0) return;
+    for (int64_t v = t.rank(); v < N; v += t.size()) haspos[v] = 0;
+    t.sync();
+    const int64_t P = team_sum<Team, int64_t>(t, sc, sm, A.n, [&](int64_t e) -> int64_t {
+        if (!(A.cost[e] > pos_tol)) return 0;
+        haspos[A.row[e]] = 1;
+        haspos[A.col[e]] = 1;
+        return 1;
+    });
+    // one scan counts both: the low 32 bits count every repulsive edge (the
+    // budget counts them all, :247), the high bits the kept ones
+    const int64_t packed = team_scan<Team, int64_t>(
+        t, sc, sm, A.n,
+        [&](int64_t e) -> int64_t {
+            if (!(A.cost[e] < thresh)) return 0;
+            return (haspos[A.row[e]] && haspos[A.col[e]]) ? (int64_t(1) << 32) + 1 : 1;
+        },
+        [&](int64_t e, int64_t pre, int64_t v) {
+            if (v >> 32) ridx[pre >> 32] = e;
+        });
+    const int64_t Rall = packed & 0xffffffffll;
+    const int64_t R = packed >> 32;
+    if (P == 0 || R == 0) {
+        sc.alg_bytes += 12.0 * (double)A.n;
+        return;
+    }
     Csr C = build_symmetric_csr(t, sc, sm, A, N, [&](int64_t e) { return A.cost[e] > pos_tol; }, false);
-    const int64_t budget = (int64_t)(int32_t)(tri_factor * (float)R);  // (:247)
+    const int64_t budget = (int64_t)(int32_t)(tri_factor * (float)Rall);  // (:247)
     tb.budget = budget < 0 ? 0 : budget;
     tb.t1 = sc.arena.take<int32_t>(tb.budget + 1);
     tb.t2 = sc.arena.take<int32_t>(tb.budget + 1);

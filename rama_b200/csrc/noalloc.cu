@@ -165,7 +165,10 @@ extern "C" int rama_solve_small_static(const int32_t *d_i, const int32_t *d_j, c
         return fail_static(RAMA_ERR_INVALID_ARG,
                            "rama_solve_small_static: invalid input (negative id, self loop, node id >= " +
                                std::to_string(RAMA_STATIC_MAX_NODES) + ", or label buffer too small)");
-    if ((ho.status & ERR_ARENA) || ho.dual_oom)
+    // a dual that ran out of scratch fell back to the trivial bound (the
+    // reference's caught bad_alloc) and the solve went on: a result, as in
+    // rama_solve; only a primal phase that ran out is an error
+    if (ho.status & ERR_ARENA)
         return fail_static(RAMA_ERR_OOM,
                            "rama_solve_small_static: the instance needs more than the fixed 32 MiB workspace "
                            "(use rama_solve)");

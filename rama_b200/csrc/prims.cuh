@@ -27,8 +27,10 @@ struct Scratch {
     int32_t *err;   // set when a bounded wait gave up (zeroed at the start of a solve)
     int parity;
     double alg_bytes;  // algorithmic bytes of the work done (team-uniform tally)
-    int64_t *prof;     // optional per-phase nanoseconds (leader only)
+    int64_t *prof;     // optional: per-phase nanoseconds [0, PH_COUNT), then per-phase
+                       // algorithmic bytes [PH_COUNT, 2 PH_COUNT) (leader only)
     uint64_t tlast;
+    double alg_last;   // alg_bytes at the last phase mark
     __device__ __forceinline__ char *next_part()
     {
         parity ^= 1;
@@ -50,6 +52,7 @@ __device__ __forceinline__ Scratch scratch_over(char *base, uint64_t bytes)
     sc.alg_bytes = 0.0;
     sc.prof = nullptr;
     sc.tlast = 0;
+    sc.alg_last = 0.0;
     sc.arena.base = base;
     sc.arena.cap = bytes - 256;
     sc.arena.lo = 2 * SCRATCH_PART_BYTES + 256;
@@ -59,9 +62,10 @@ __device__ __forceinline__ Scratch scratch_over(char *base, uint64_t bytes)
     return sc;
 }
 
-// Phase timing: the team leader charges the time since the last mark to
-// `phase`.  Marks sit right after team syncs, so a phase's time is the span
-// in which the whole team worked on it.
+// Phase timing: the team leader charges the time since the last mark, and
+// the algorithmic bytes tallied since then, to `phase`.  Marks sit right
+// after team syncs, so a phase's time is the span in which the whole team
+// worked on it.
 enum Phase : int {
     PH_INIT = 0,
     PH_CYCLES = 1,
@@ -88,8 +92,10 @@ __device__ __forceinline__ void prof_mark(const Team &t, Scratch &sc, int phase)
     if (sc.prof && t.leader()) {
         uint64_t now = prof_now();
         sc.prof[phase] += (int64_t)(now - sc.tlast);
+        sc.prof[PH_COUNT + phase] += (int64_t)(sc.alg_bytes - sc.alg_last);
         sc.tlast = now;
     }
+    sc.alg_last = sc.alg_bytes;
 }
 
 // ---------------------------------------------------------------------------

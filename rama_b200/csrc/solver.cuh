@@ -35,7 +35,7 @@ struct Instance {
     int64_t labels_cap;
     int32_t *timeline;       // optional: rounds x num_labels
     int64_t timeline_cap;    // entries
-    int64_t *prof;           // optional: PH_COUNT nanosecond counters
+    int64_t *prof;           // optional: PH_COUNT nanosecond counters, then PH_COUNT byte counters
     char *ws;                // workspace slice of this instance (CTA solves)
     uint64_t ws_bytes;
     // outputs

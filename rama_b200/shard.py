@@ -52,17 +52,30 @@ def solve_batch_sharded(batch: "I.Batch", mode: str = "PD", rank: int = 0, world
                 raise RuntimeError(f"batch solve failed on rank {rank}: status {status.tolist()}")
             return res
 
-    part = solve(I.pack([batch.instance(k) for k in mine]), mode) if mine else []
-    local = [(k, np.asarray(lab), float(lb)) for k, (lab, lb) in zip(mine, part)]
+    # A rank whose solve fails still takes part in the gather (otherwise the
+    # other ranks would wait in it for ever): it sends its error instead of
+    # results, and every rank raises after the gather.
+    error = None
+    local: list = []
+    try:
+        part = solve(I.pack([batch.instance(k) for k in mine]), mode) if mine else []
+        local = [(k, np.asarray(lab), float(lb)) for k, (lab, lb) in zip(mine, part)]
+    except Exception as e:  # noqa: BLE001 -- re-raised on every rank below
+        if world == 1:
+            raise
+        error = f"rank {rank}: {type(e).__name__}: {e}"
     if world == 1:
-        gathered = [local]
+        gathered = [(None, local)]
     else:
         import torch.distributed as dist
 
         gathered = [None] * world
-        dist.all_gather_object(gathered, local, group=group)
+        dist.all_gather_object(gathered, (error, local), group=group)
+    failed = [err for err, _ in gathered if err is not None]
+    if failed:
+        raise RuntimeError("sharded batch solve failed: " + "; ".join(failed))
     out: List[Optional[Tuple[np.ndarray, float]]] = [None] * batch.count
-    for lst in gathered:
+    for _, lst in gathered:
         for k, lab, lb in lst:
             out[k] = (lab, lb)
     if any(x is None for x in out):

@@ -69,6 +69,42 @@ def test_two_gloo_ranks_gather_the_one_process_result(tmp_path):
             assert np.array_equal(got[f"lab{k}"], lab)
 
 
+def _failing_solve(b, mode):
+    raise RuntimeError("planted failure")
+
+
+def _rank_main_one_fails(rank, world, port, outdir):
+    import torch.distributed as dist
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    from datetime import timedelta
+
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=timedelta(seconds=60))
+    try:
+        solve = _failing_solve if rank == 1 else _oracle_batch_solve
+        try:
+            shard.solve_batch_sharded(_batch(), "PD", rank, world, solve=solve)
+            msg = "no error"
+        except RuntimeError as e:
+            msg = str(e)
+        with open(os.path.join(outdir, f"r{rank}.txt"), "w") as f:
+            f.write(msg)
+    finally:
+        dist.destroy_process_group()
+
+
+def test_a_failing_rank_raises_on_every_rank(tmp_path):
+    """Rank 1's solve raises; both ranks leave the gather and raise an error
+    that names rank 1, instead of rank 0 waiting in the gather."""
+    import torch.multiprocessing as mp
+
+    mp.spawn(_rank_main_one_fails, args=(2, _free_port(), str(tmp_path)), nprocs=2, join=True)
+    for r in range(2):
+        msg = (tmp_path / f"r{r}.txt").read_text()
+        assert "rank 1" in msg and "planted failure" in msg, msg
+
+
 @pytest.mark.gpu
 def test_one_rank_solves_the_batch_on_the_gpu(oracle):
     b = _batch()

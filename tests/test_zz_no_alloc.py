@@ -65,3 +65,44 @@ def test_static_rejects_oversized_instance():
                                              8, C.byref(nl), C.byref(lb), None)
     assert rc == _lib.RAMA_ERR_INVALID_ARG
     assert b"exceed the limit of 30000" in _lib.load().rama_last_error()
+
+
+def test_static_rejects_node_id_beyond_limit():
+    """A node id of RAMA_STATIC_MAX_NODES (65,536) is refused on the device
+    before the solve starts."""
+    import torch
+
+    i = np.array([0, 1, 2], np.int32)
+    j = np.array([1, 2, 65536], np.int32)
+    c = np.array([1.0, -1.0, 0.5], np.float32)
+    d_i, d_j, d_c = (torch.from_numpy(x).cuda() for x in (i, j, c))
+    d_lab = torch.zeros(65537, dtype=torch.int32, device="cuda")
+    rc, nl, _ = _static(d_i, d_j, d_c, 3, _lib.options("PD"), d_lab)
+    assert rc == _lib.RAMA_ERR_INVALID_ARG
+    assert nl == 0
+    assert b"65536" in _lib.load().rama_last_error()
+
+
+@pytest.mark.parametrize("mode", ("PD", "PD+"))
+def test_static_near_the_edge_limit(mode):
+    """An instance just under the 30,000-edge limit fits the fixed array and
+    gives rama_solve's result, twice in a row."""
+    import torch
+
+    from rama_b200.solver import Solver
+
+    i, j, c = instances.grid2d(122, 123, seed=37)  # 29,767 edges
+    assert 29000 < len(c) <= 30000
+    d_i, d_j, d_c = (torch.from_numpy(np.ascontiguousarray(x)).cuda() for x in (i, j, c))
+    N = int(max(i.max(), j.max())) + 1
+    s = Solver(0)
+    ref_lab, ref_lb = s.solve_device(d_i, d_j, d_c, mode=mode, team=1)
+    ref_lab = ref_lab.cpu().numpy()
+    assert s.stats().workspace_peak < (32 << 20) - 4096
+    for _ in range(2):
+        d_lab = torch.full((N,), -7, dtype=torch.int32, device="cuda")
+        rc, nl, lb = _static(d_i, d_j, d_c, len(c), _lib.options(mode), d_lab)
+        assert rc == 0, _lib.load().rama_last_error()
+        assert nl == N
+        assert lb == ref_lb
+        assert np.array_equal(d_lab.cpu().numpy(), ref_lab)
