@@ -292,6 +292,8 @@ def run_ours(args, rank, world, local):
     }
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, mode)
+        if "fp64_error" in line["cpu_baseline"]:
+            line["lb_error_vs_fp64"] = line["cpu_baseline"]["fp64_error"]
     return line
 
 
@@ -515,7 +517,23 @@ def cpu_baseline(cfg, mode):
             "gaec": {"value": edges / (t3 - t2), "unit": "edges/s", "cores": 1,
                      "what": "project-written sequential greedy additive edge contraction + union-find",
                      "objective": gaec_obj, "rama_oracle_objective": rama_obj},
-            "cpu_model": cpu_model(), "host_cores": os.cpu_count()}
+            "cpu_model": cpu_model(), "host_cores": os.cpu_count(),
+            **({"fp64_error": fp64_error(O, i, j, c)} if mode == "D" else {})}
+
+
+def fp64_error(O, i, j, c):
+    """Error of the bound against the FP64 oracle on the sample: the same
+    triangle selection with every cost, message and bound in double.  The GPU
+    solve of the sample runs through the C ABI like the timed solves."""
+    from rama_b200.solver import Solver
+
+    t0 = time.perf_counter()
+    lb64 = O.dual_lb_f64(i, j, c, "D")
+    t1 = time.perf_counter()
+    _, lb_gpu, _ = Solver(0).solve(i, j, c, mode="D")
+    return {"edges": len(c), "lb_gpu": lb_gpu, "lb_fp64": lb64, "abs": abs(lb_gpu - lb64),
+            "rel": abs(lb_gpu - lb64) / max(1.0, abs(lb64)), "fp64_oracle_s": round(t1 - t0, 2),
+            "what": "GPU: FP32 messages, compensated FP64 bound; oracle: all FP64, same triangle selection"}
 
 
 def run_reference_many(args, local, R):

@@ -107,6 +107,9 @@ def lib():
         L.orc_mp_info.argtypes = [C.c_void_p, C.POINTER(_i64), C.POINTER(_i64)]
         L.orc_mp_copy_edges.argtypes = [C.c_void_p, _i32p, _i32p, _f32p, _i32p]
         L.orc_mp_copy_triangles.argtypes = [C.c_void_p] + [_i32p] * 3 + [_f32p] * 3 + [_i32p] * 3
+        L.orc_dual_lb_f64.restype = C.c_int
+        L.orc_dual_lb_f64.argtypes = [_i64, _i32p, _i32p, _f32p, C.c_int32, C.c_int32, C.c_float, C.c_int32,
+                                      C.c_float, C.POINTER(C.c_double)]
         L.orc_dual_solver.restype = C.c_double
         L.orc_dual_solver.argtypes = [C.POINTER(_G), C.c_int32, C.c_int32, C.c_float, C.c_int32, C.c_float,
                                       C.POINTER(_i64)]
@@ -308,6 +311,19 @@ def dual_solver(g: Graph, max_len, num_iter, tri_factor=2.0, num_outer=1, tol=1e
     g.ptr = None  # ownership moved (the old graph was freed if replaced)
     del ptr, holder
     return Graph(newp), lb, nt.value
+
+
+def dual_lb_f64(i, j, c, mode="D", **kw):
+    """The bound of the dual phase of `mode` computed by the FP64 oracle: the
+    same triangle selection, every cost, message and bound in double."""
+    o = opts(mode, **kw)
+    i, j, c = _a32(i), _a32(j), _f32(c)
+    lb = C.c_double(0)
+    rc = lib().orc_dual_lb_f64(len(c), i, j, c, o.max_cycle_length_lb, o.num_dual_itr_lb, o.tri_memory_factor,
+                               o.num_outer_itr_dual, 1e-4, C.byref(lb))
+    if rc != 0:
+        raise RuntimeError(f"FP64 dual oracle failed with status {rc}")
+    return lb.value
 
 
 def opts(mode=None, **kw):

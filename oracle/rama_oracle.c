@@ -18,9 +18,15 @@
  *  C3  sums of parallel edges after contraction and of messages arriving at
  *      an edge use RSUM: FP64, 32 lane-strided partial sums in element order,
  *      pairwise tree over lanes, rounded once to float.
- *  C4  the triangle budget keeps the FIRST `budget` emissions in canonical
- *      order (rep edge order, then neighbour/expansion order, then common
- *      neighbour ascending); the reference keeps whichever its atomics admit.
+ *  C4  the triangle budget: expansions (a rep edge; a rep edge and a
+ *      neighbour; a rep edge and two neighbours) are taken in canonical order
+ *      in chunks of 2^24, each emitting its triangles in a fixed order.  A
+ *      chunk whose emissions exceed the room left keeps them round-robin:
+ *      the first K emissions of every expansion, K as large as fits, and one
+ *      more for the first expansions (in order) that have one, until the room
+ *      is full.  The reference keeps whichever emissions its atomics admit;
+ *      with all its threads resident that is close to round-robin over rep
+ *      edges, which keeps some triangles of every conflicted edge.
  *  C5  Boruvka picks per super-vertex the lexicographic minimum of
  *      (-weight, target super-vertex, edge id); the reference's reduce-by-key
  *      only fixes (-weight, target).
@@ -1238,6 +1244,122 @@ static int64_t tri_normalize(int32_t *buf, int64_t n)
         }                                                                          \
     } while (0)
 
+/* Expansions of one stage of the cycle search and the triangles each emits
+ * (3-cycles :31-61, 4-cycles :63-101, 5-cycles :103-148).  emit_first()
+ * emits the first `keep` emissions of expansion x, in the reference's order. */
+typedef struct {
+    int kind; /* 3, 4 or 5 */
+    const csr_t *P;
+    const int32_t *rr, *rc;
+    const int64_t *xo; /* kinds 4, 5: first expansion of each rep edge (R + 1) */
+    int64_t R;
+} stage_t;
+
+static void stage_locate(const stage_t *S, int64_t x, int64_t *r, int64_t *loc)
+{
+    if (S->kind == 3) {
+        *r = x;
+        *loc = 0;
+        return;
+    }
+    int64_t lo = 0, hi = S->R; /* largest r with xo[r] <= x */
+    while (lo < hi) {
+        int64_t mid = (lo + hi + 1) >> 1;
+        if (S->xo[mid] <= x)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    *r = lo;
+    *loc = x - S->xo[lo];
+}
+
+/* emissions of expansion x (keep < 0: count only, emit nothing) */
+static int64_t stage_expand(const stage_t *S, int64_t x, int64_t keep, tri_emit_t *T)
+{
+    int64_t r, loc, n = 0;
+    stage_locate(S, x, &r, &loc);
+    const csr_t *P = S->P;
+    int32_t v1 = S->rr[r], v2 = S->rc[r];
+#define EMIT(a, b, c)                                   \
+    do {                                                \
+        if (keep >= 0 && n < keep) tri_emit(T, a, b, c); \
+        n++;                                            \
+    } while (0)
+    if (S->kind == 3) {
+        FOR_COMMON(P->off, P->adj, v1, v2, mid, EMIT(v1, v2, mid));
+    } else if (S->kind == 4) {
+        int32_t n1 = P->adj[P->off[v1] + (int32_t)loc];
+        FOR_COMMON(P->off, P->adj, n1, v2, mid, {
+            EMIT(v1, v2, n1);
+            EMIT(v2, n1, mid);
+        });
+    } else {
+        int64_t d1 = P->off[v1 + 1] - P->off[v1];
+        int32_t n1 = P->adj[P->off[v1] + (int32_t)(loc % d1)];
+        int32_t n2 = P->adj[P->off[v2] + (int32_t)(loc / d1)];
+        if (n1 != n2) {
+            FOR_COMMON(P->off, P->adj, n1, n2, mid, {
+                EMIT(v1, v2, n1);
+                EMIT(v2, n1, mid);
+                EMIT(v2, mid, n2);
+            });
+        }
+    }
+#undef EMIT
+    return n;
+}
+
+#define STAGE_CHUNK ((int64_t)1 << 24)
+
+/* One stage over X expansions in chunks; a chunk that does not fit the room
+ * left keeps its emissions round-robin (C4) and fills the budget. */
+static void stage_run(const stage_t *S, int64_t X, tri_emit_t *T)
+{
+    int64_t *m = NEW(int64_t, X < STAGE_CHUNK ? X + 1 : STAGE_CHUNK);
+    for (int64_t x0 = 0; x0 < X && T->count <= T->budget; x0 += STAGE_CHUNK) {
+        int64_t xn = X - x0 < STAGE_CHUNK ? X - x0 : STAGE_CHUNK;
+        int64_t M = 0, mx = 0;
+        for (int64_t q = 0; q < xn; ++q) {
+            m[q] = stage_expand(S, x0 + q, -1, T);
+            M += m[q];
+            if (m[q] > mx) mx = m[q];
+        }
+        int64_t rem = T->budget - T->count;
+        if (M <= rem) {
+            for (int64_t q = 0; q < xn; ++q)
+                if (m[q]) stage_expand(S, x0 + q, m[q], T);
+            continue;
+        }
+        /* largest K with sum_q min(m_q, K) <= rem */
+        int64_t lo = 0, hi = mx;
+        while (lo < hi) {
+            int64_t K = (lo + hi + 1) >> 1, s = 0;
+            for (int64_t q = 0; q < xn; ++q) s += m[q] < K ? m[q] : K;
+            if (s <= rem)
+                lo = K;
+            else
+                hi = K - 1;
+        }
+        const int64_t K = lo;
+        int64_t sK = 0;
+        for (int64_t q = 0; q < xn; ++q) sK += m[q] < K ? m[q] : K;
+        const int64_t extra = rem - sK;
+        int64_t big = 0;
+        for (int64_t q = 0; q < xn; ++q) {
+            int64_t keep = m[q] < K ? m[q] : K;
+            if (m[q] > K) {
+                if (big < extra) keep++;
+                big++;
+            }
+            if (keep) stage_expand(S, x0 + q, keep, T);
+        }
+        T->count = T->budget + 1; /* the reference's counter has overflowed */
+        T->full = 1;
+    }
+    free(m);
+}
+
 int orc_conflicted_cycles(const orc_graph *A, int32_t max_len, float tri_factor, float tol_ratio, int32_t *tri_out,
                           int64_t tri_cap, int64_t *num_out, int64_t *raw_count)
 {
@@ -1282,43 +1404,28 @@ int orc_conflicted_cycles(const orc_graph *A, int32_t max_len, float tri_factor,
     T.budget = budget;
     T.count = 0;
     T.full = 0;
-    /* find_triangles_parallel (:31-61) */
-    for (int64_t r = 0; r < R && !T.full; ++r) {
-        int32_t v1 = rr[r], v2 = rc[r];
-        FOR_COMMON(P.off, P.adj, v1, v2, mid, tri_emit(&T, v1, v2, mid));
-    }
+    int64_t *xo = NEW(int64_t, R + 1);
+    stage_t S = {3, &P, rr, rc, xo, R};
+    /* find_triangles_parallel (:31-61): one expansion per rep edge */
+    stage_run(&S, R, &T);
     if (max_len >= 4 && T.count < budget) {
         T.count = tri_normalize(T.buf, T.count);
-        /* find_quadrangles_parallel (:63-101) */
-        for (int64_t r = 0; r < R && !T.full; ++r) {
-            int32_t v1 = rr[r], v2 = rc[r];
-            for (int32_t k1 = P.off[v1]; k1 < P.off[v1 + 1] && !T.full; ++k1) {
-                int32_t n1 = P.adj[k1];
-                FOR_COMMON(P.off, P.adj, n1, v2, mid, {
-                    tri_emit(&T, v1, v2, n1);
-                    tri_emit(&T, v2, n1, mid);
-                });
-            }
-        }
+        /* find_quadrangles_parallel (:63-101): a rep edge and a neighbour of its row */
+        xo[0] = 0;
+        for (int64_t r = 0; r < R; ++r) xo[r + 1] = xo[r] + (P.off[rr[r] + 1] - P.off[rr[r]]);
+        S.kind = 4;
+        stage_run(&S, xo[R], &T);
     }
     if (max_len >= 5 && T.count < budget) {
         T.count = tri_normalize(T.buf, T.count);
-        /* find_pentagons_parallel (:103-148) */
-        for (int64_t r = 0; r < R && !T.full; ++r) {
-            int32_t v1 = rr[r], v2 = rc[r];
-            int64_t d1 = P.off[v1 + 1] - P.off[v1], d2 = P.off[v2 + 1] - P.off[v2];
-            for (int64_t loc = 0; loc < d1 * d2 && !T.full; ++loc) {
-                int32_t n1 = P.adj[P.off[v1] + (int32_t)(loc % d1)];
-                int32_t n2 = P.adj[P.off[v2] + (int32_t)(loc / d1)];
-                if (n1 == n2) continue;
-                FOR_COMMON(P.off, P.adj, n1, n2, mid, {
-                    tri_emit(&T, v1, v2, n1);
-                    tri_emit(&T, v2, n1, mid);
-                    tri_emit(&T, v2, mid, n2);
-                });
-            }
-        }
+        /* find_pentagons_parallel (:103-148): a rep edge and a neighbour of each end */
+        xo[0] = 0;
+        for (int64_t r = 0; r < R; ++r)
+            xo[r + 1] = xo[r] + (int64_t)(P.off[rr[r] + 1] - P.off[rr[r]]) * (int64_t)(P.off[rc[r] + 1] - P.off[rc[r]]);
+        S.kind = 5;
+        stage_run(&S, xo[R], &T);
     }
+    free(xo);
     int64_t keep = T.count < budget ? T.count : budget;
     if (T.count > budget) g_truncations++;
     if (keep > tri_cap) keep = tri_cap;
@@ -1693,6 +1800,186 @@ double orc_dual_solver(orc_graph **pA, int32_t max_len, int32_t num_iter, float 
     }
     if (num_triangles_last) *num_triangles_last = nt;
     return fin;
+}
+
+/* ------------------------------------------------------------------------ */
+/* FP64 oracle of the dual, for the error report of the FP32 messages        */
+/* ------------------------------------------------------------------------ */
+/* The dual solver (src/dual_solver.cu:7-63) with every cost, message and
+ * bound in double.  The triangle search runs on the costs rounded to float:
+ * it only selects triangles (thresholds, counts), and the FP32 solve makes the
+ * same selection.  Message passing (src/multicut_message_passing.cu:218-348)
+ * and the bound (:178-216) are evaluated in FP64 throughout. */
+static inline double tri_lb64(double c12, double c13, double c23)
+{
+    double lb = 0.0;
+    lb = fmin(lb, c12 + c13);
+    lb = fmin(lb, c12 + c23);
+    lb = fmin(lb, c13 + c23);
+    lb = fmin(lb, c12 + c13 + c23);
+    return lb;
+}
+
+static inline double min_marginal64(double x, double y, double z)
+{
+    double mm1 = fmin(x + y + z, fmin(x + y, x + z));
+    double yz = y + z;
+    double mm0 = yz > 0.0 ? 0.0 : yz;
+    return mm1 - mm0;
+}
+
+typedef struct {
+    double *cost, *c12, *c13, *c23, *diff;
+} mp64_t;
+
+static double mp64_lower_bound(const orc_mp *mp, const mp64_t *d)
+{
+    csum_acc a;
+    cacc_init(&a);
+    for (int64_t e = 0; e < mp->E; ++e) cacc_push(&a, d->cost[e] < 0.0 ? d->cost[e] : 0.0);
+    double le = cacc_finish(&a);
+    cacc_init(&a);
+    for (int64_t t = 0; t < mp->T; ++t) cacc_push(&a, tri_lb64(d->c12[t], d->c13[t], d->c23[t]));
+    return le + cacc_finish(&a);
+}
+
+static void mp64_iteration(const orc_mp *mp, mp64_t *d)
+{
+    for (int64_t t = 0; t < mp->T; ++t) {
+        d->c12[t] += d->cost[mp->e12[t]] / (double)mp->cnt[mp->e12[t]];
+        d->c13[t] += d->cost[mp->e13[t]] / (double)mp->cnt[mp->e13[t]];
+        d->c23[t] += d->cost[mp->e23[t]] / (double)mp->cnt[mp->e23[t]];
+    }
+    for (int64_t e = 0; e < mp->E; ++e)
+        if (mp->cnt[e] > 0) d->cost[e] = 0.0;
+    const double third = 1.0 / 3.0, half = 1.0 / 2.0;
+    for (int64_t t = 0; t < mp->T; ++t) {
+        double t12 = d->c12[t], t13 = d->c13[t], t23 = d->c23[t], e12 = 0.0, e13 = 0.0, e23 = 0.0, mm;
+        mm = min_marginal64(t12, t13, t23);
+        t12 -= third * mm;
+        e12 += third * mm;
+        mm = min_marginal64(t13, t12, t23);
+        t13 -= half * mm;
+        e13 += half * mm;
+        mm = min_marginal64(t23, t12, t13);
+        t23 -= mm;
+        e23 += mm;
+        mm = min_marginal64(t12, t13, t23);
+        t12 -= half * mm;
+        e12 += half * mm;
+        mm = min_marginal64(t13, t12, t23);
+        t13 -= mm;
+        e13 += mm;
+        mm = min_marginal64(t12, t13, t23);
+        t12 -= mm;
+        e12 += mm;
+        d->c12[t] = t12;
+        d->c13[t] = t13;
+        d->c23[t] = t23;
+        d->diff[3 * t] = e12;
+        d->diff[3 * t + 1] = e13;
+        d->diff[3 * t + 2] = e23;
+    }
+    for (int64_t e = 0; e < mp->E; ++e)
+        for (int32_t k = mp->inc_off[e]; k < mp->inc_off[e + 1]; ++k) d->cost[e] += d->diff[mp->inc[k]];
+}
+
+/* one cycle length: the graph *pA carries float costs, *pcd the same costs
+ * in double; both are replaced by the reparametrised graph */
+static double dual_update_cycle_length_f64(orc_graph **pA, double **pcd, int32_t c, int32_t num_iter,
+                                           float tri_factor, float tol, int64_t *num_tri)
+{
+    orc_graph *A = *pA;
+    const double *cd = *pcd;
+    csum_acc acc;
+    int64_t cap = (int64_t)(tri_factor * (double)A->n) + 8;
+    int32_t *tri = NEW(int32_t, 3 * cap);
+    int64_t num = 0, raw = 0;
+    orc_conflicted_cycles(A, c, tri_factor, tol, tri, cap, &num, &raw);
+    *num_tri = raw;
+    if (raw == 0) {
+        free(tri);
+        cacc_init(&acc);
+        for (int64_t e = 0; e < A->n; ++e) cacc_push(&acc, cd[e] < 0.0 ? cd[e] : 0.0);
+        return cacc_finish(&acc);
+    }
+    int32_t *t1 = NEW(int32_t, num + 1), *t2 = NEW(int32_t, num + 1), *t3 = NEW(int32_t, num + 1);
+    for (int64_t k = 0; k < num; ++k) {
+        t1[k] = tri[3 * k];
+        t2[k] = tri[3 * k + 1];
+        t3[k] = tri[3 * k + 2];
+    }
+    free(tri);
+    orc_mp *mp = orc_mp_create(A, t1, t2, t3, num);
+    free(t1);
+    free(t2);
+    free(t3);
+    /* double costs of the merged edge list: A's own edges keep theirs, the
+     * added triangle chords start at 0 */
+    mp64_t d;
+    d.cost = NEW(double, mp->E + 1);
+    d.c12 = (double *)xcalloc((size_t)mp->T + 1, sizeof(double));
+    d.c13 = (double *)xcalloc((size_t)mp->T + 1, sizeof(double));
+    d.c23 = (double *)xcalloc((size_t)mp->T + 1, sizeof(double));
+    d.diff = NEW(double, 3 * mp->T + 1);
+    int32_t nmax = graph_max_dim(A);
+    for (int64_t e = 0; e < mp->E; ++e) nmax = imax(nmax, mp->col[e] + 1);
+    int32_t *aoff = NEW(int32_t, nmax + 2);
+    orc_compute_offsets(A->row, A->n, nmax, aoff);
+    for (int64_t e = 0; e < mp->E; ++e) {
+        int64_t x = mp->row[e] < nmax ? edge_find(aoff, A->col, mp->row[e], mp->col[e]) : -1;
+        d.cost[e] = x >= 0 ? cd[x] : 0.0;
+    }
+    free(aoff);
+    double prev = 0.0;
+    for (int32_t it = 0; it < num_iter; ++it) {
+        double lb = mp64_lower_bound(mp, &d);
+        if (it > 0 && (lb - prev) < 1e-3) break;
+        mp64_iteration(mp, &d);
+        prev = lb;
+    }
+    double fin = mp64_lower_bound(mp, &d);
+    float *cf = NEW(float, mp->E + 1);
+    for (int64_t e = 0; e < mp->E; ++e) cf[e] = (float)d.cost[e];
+    orc_graph *B = orc_graph_from_sorted(mp->E, mp->row, mp->col, cf);
+    orc_mp_free(mp);
+    free(cf);
+    free(d.c12);
+    free(d.c13);
+    free(d.c23);
+    free(d.diff);
+    orc_graph_free(A);
+    free(*pcd);
+    *pA = B;
+    *pcd = d.cost;
+    return fin;
+}
+
+int orc_dual_lb_f64(int64_t n, const int32_t *i, const int32_t *j, const float *c, int32_t max_len, int32_t num_iter,
+                    float tri_factor, int32_t num_outer, float tol, double *lb)
+{
+    orc_graph *A = orc_graph_from_edges(n, i, j, c);
+    double *cd = NEW(double, A->n + 1);
+    for (int64_t e = 0; e < A->n; ++e) cd[e] = (double)A->cost[e];
+    double fin = 0.0, prev = 0.0;
+    if (max_len < 3 || num_iter == 0 || num_outer == 0) {
+        csum_acc acc;
+        cacc_init(&acc);
+        for (int64_t e = 0; e < A->n; ++e) cacc_push(&acc, cd[e] < 0.0 ? cd[e] : 0.0);
+        fin = cacc_finish(&acc);
+    } else {
+        int64_t nt = 0;
+        for (int32_t o = 0; o < num_outer; ++o) {
+            for (int32_t cl = 3; cl <= max_len; ++cl)
+                fin = dual_update_cycle_length_f64(&A, &cd, cl, num_iter, tri_factor, tol, &nt);
+            if (nt == 0 || (o > 0 && (fin - prev) < 1e-3)) break;
+            prev = fin;
+        }
+    }
+    free(cd);
+    orc_graph_free(A);
+    *lb = fin;
+    return ORC_OK;
 }
 
 /* ------------------------------------------------------------------------ */

@@ -106,6 +106,11 @@ int orc_woc_ex(const orc_graph *A, int32_t *map_out, int64_t *map_size, int32_t 
 int orc_conflicted_cycles(const orc_graph *A, int32_t max_cycle_length, float tri_memory_factor, float tol_ratio,
                           int32_t *tri_out, int64_t tri_cap, int64_t *num_out, int64_t *raw_count);
 
+/* FP64 oracle of the dual solver: the same triangle selection, every cost,
+ * message and bound in double (for reporting the error of the FP32 messages) */
+int orc_dual_lb_f64(int64_t n, const int32_t *i, const int32_t *j, const float *c, int32_t max_len, int32_t num_iter,
+                    float tri_factor, int32_t num_outer, float tol, double *lb);
+
 /* ---- message passing ---- */
 typedef struct orc_mp orc_mp;
 orc_mp *orc_mp_create(const orc_graph *A, const int32_t *t1, const int32_t *t2, const int32_t *t3, int64_t T);

@@ -1,8 +1,12 @@
 // cycles.cuh -- conflicted 3/4/5-cycle search on the CSR of attractive edges
 // (src/conflicted_cycles_cuda.cu:13-343).  Each conflicted cycle is emitted
-// as triangles; the budget keeps the first `budget` emissions in canonical
-// order (rep edge, neighbour/expansion index, common neighbour ascending),
-// computed by count -> scan -> write over chunks of expansions.
+// as triangles.  Expansions (a rep edge; a rep edge and a neighbour; a rep
+// edge and two neighbours) are taken in canonical order in chunks of 2^24,
+// each emitting its triangles in the reference's order; a chunk whose
+// emissions exceed the room left in the budget keeps them round-robin: the
+// first K emissions of every expansion (K as large as fits) and one more for
+// the first expansions that have one, until the budget is full.  Computed by
+// count -> K -> scan -> write.
 #pragma once
 #include "graph.cuh"
 
@@ -27,12 +31,13 @@ __device__ __forceinline__ int count_common(const int32_t *adj, int32_t a0, int3
     return c;
 }
 
+// calls f(mid) for the common neighbours in ascending order while f returns true
 template <class F>
 __device__ __forceinline__ void for_common(const int32_t *adj, int32_t a0, int32_t a1, int32_t b0, int32_t b1, F f)
 {
     while (a0 < a1 && b0 < b1) {
         int32_t x = adj[a0], y = adj[b0];
-        if (x == y) f(x);
+        if (x == y && !f(x)) return;
         a0 += (x <= y);
         b0 += (y <= x);
     }
@@ -143,11 +148,14 @@ __device__ __forceinline__ int64_t expansion_owner(const int64_t *xo, int64_t R,
     return lo;
 }
 
+// emit(r, loc, pos, keep) writes the first `keep` emissions of an expansion
+// at pos, pos + 1, ...
 template <class Team, class Count, class Emit>
 __device__ void expansion_stage(const Team &t, Scratch &sc, char *sm, TriBuf &tb, const int64_t *xo, int64_t R,
                                 int64_t X, Count cnt, Emit emit)
 {
     const int64_t CH = int64_t(1) << 24;
+    const int64_t KALL = int64_t(1) << 40;  // no truncation: every emission is kept
     uint64_t m = sc.arena.mark();
     int32_t *ccount = sc.arena.take<int32_t>(CH < X ? CH : X + 1);
     int64_t *cbase = sc.arena.take<int64_t>((CH < X ? CH : X) + 1);
@@ -172,13 +180,47 @@ __device__ void expansion_stage(const Team &t, Scratch &sc, char *sm, TriBuf &tb
             ccount[q] = cnt(r, xo ? x - xo[r] : 0);
         }
         t.sync();
-        const int64_t tot = team_scan<Team, int64_t>(
-            t, sc, sm, xn, [&](int64_t q) -> int64_t { return ccount[q]; },
-            [&](int64_t q, int64_t pre, int64_t) { cbase[q] = pre; });
         const int64_t start = tb.count;
+        const int64_t rem = tb.budget - start;
+        const int64_t tot = team_sum<Team, int64_t>(t, sc, sm, xn, [&](int64_t q) -> int64_t { return ccount[q]; });
+        // round-robin when the chunk does not fit: the largest K with
+        // sum_q min(count_q, K) <= rem, and `extra` expansions keep one more
+        int64_t K = KALL, extra = 0;
+        if (tot > rem) {
+            const int32_t mx = team_max<Team, int32_t>(t, sc, sm, xn, 0, [&](int64_t q) { return ccount[q]; });
+            int64_t lo = 0, hi = mx, slo = 0;
+            for (int guard = 0; lo < hi && guard < 40; ++guard) {
+                const int64_t k = (lo + hi + 1) >> 1;
+                const int64_t s = team_sum<Team, int64_t>(t, sc, sm, xn, [&](int64_t q) -> int64_t {
+                    const int64_t c = ccount[q];
+                    return c < k ? c : k;
+                });
+                if (s <= rem) {
+                    lo = k;
+                    slo = s;
+                } else {
+                    hi = k - 1;
+                }
+            }
+            K = lo;
+            extra = rem - slo;
+        }
+        // positions: one scan of (kept below K) << 25 | (has more than K);
+        // count_q is replaced by the number it keeps
+        team_scan<Team, int64_t>(
+            t, sc, sm, xn,
+            [&](int64_t q) -> int64_t {
+                const int64_t c = ccount[q];
+                return ((c < K ? c : K) << 25) | (c > K ? 1 : 0);
+            },
+            [&](int64_t q, int64_t pre, int64_t v) {
+                const int64_t pmin = pre >> 25, pbig = pre & ((int64_t(1) << 25) - 1);
+                cbase[q] = pmin + (pbig < extra ? pbig : extra);
+                ccount[q] = (int32_t)((v >> 25) + ((v & 1) && pbig < extra ? 1 : 0));
+            });
         for (int64_t qb = (int64_t)team_warp(t) * 32; qb < xn; qb += (int64_t)team_nwarps(t) * 32) {
             const int64_t q = qb + lane_id();
-            const bool work = q < xn && ccount[q] != 0 && start + cbase[q] < tb.budget;
+            const bool work = q < xn && ccount[q] != 0;
             if (!__any_sync(FULL, work)) continue;
             int64_t r0 = lane_id() == 0 ? expansion_owner(xo, R, x0 + qb) : 0;
             r0 = __shfl_sync(FULL, r0, 0);
@@ -190,11 +232,10 @@ __device__ void expansion_stage(const Team &t, Scratch &sc, char *sm, TriBuf &tb
                 while (r < R && xo[r + 1] <= x && ++steps <= 64) ++r;
                 if (steps > 64) r = expansion_owner(xo, R, x);
             }
-            emit(r, xo ? x - xo[r] : 0, start + cbase[q]);
+            emit(r, xo ? x - xo[r] : 0, start + cbase[q], (int64_t)ccount[q]);
         }
         t.sync();
-        tb.count = start + tot;
-        if (tb.count > tb.budget) tb.count = tb.budget + 1;
+        tb.count = tot <= rem ? start + tot : tb.budget + 1;
     }
     sc.arena.release(m);
 }
@@ -268,11 +309,12 @@ __device__ void conflicted_cycles(const Team &t, Scratch &sc, char *sm, const Gr
                 int32_t v1 = rv1(r), v2 = rv2(r);
                 return count_common(adj, off[v1], off[v1 + 1], off[v2], off[v2 + 1]);
             },
-            [&](int64_t r, int64_t, int64_t pos) {
+            [&](int64_t r, int64_t, int64_t pos, int64_t keep) {
                 int32_t v1 = rv1(r), v2 = rv2(r);
+                int64_t e = 0;
                 for_common(adj, off[v1], off[v1 + 1], off[v2], off[v2 + 1], [&](int32_t mid) {
-                    write_tri(T, pos, v1, v2, mid);
-                    ++pos;
+                    write_tri(T, pos + e, v1, v2, mid);
+                    return ++e < keep;
                 });
             });
     }
@@ -292,13 +334,15 @@ __device__ void conflicted_cycles(const Team &t, Scratch &sc, char *sm, const Gr
                 int32_t n1 = adj[off[v1] + loc];
                 return 2 * count_common(adj, off[n1], off[n1 + 1], off[v2], off[v2 + 1]);
             },
-            [&](int64_t r, int64_t loc, int64_t pos) {
+            [&](int64_t r, int64_t loc, int64_t pos, int64_t keep) {
                 int32_t v1 = rv1(r), v2 = rv2(r);
                 int32_t n1 = adj[off[v1] + loc];
+                int64_t e = 0;
                 for_common(adj, off[n1], off[n1 + 1], off[v2], off[v2 + 1], [&](int32_t mid) {
-                    write_tri(T, pos, v1, v2, n1);
-                    write_tri(T, pos + 1, v2, n1, mid);
-                    pos += 2;
+                    write_tri(T, pos + e, v1, v2, n1);
+                    if (++e >= keep) return false;
+                    write_tri(T, pos + e, v2, n1, mid);
+                    return ++e < keep;
                 });
             });
     }
@@ -325,16 +369,20 @@ __device__ void conflicted_cycles(const Team &t, Scratch &sc, char *sm, const Gr
                 if (n1 == n2) return 0;
                 return 3 * count_common(adj, off[n1], off[n1 + 1], off[n2], off[n2 + 1]);
             },
-            [&](int64_t r, int64_t loc, int64_t pos) {
+            [&](int64_t r, int64_t loc, int64_t pos, int64_t keep) {
                 int32_t v1 = rv1(r), v2 = rv2(r);
                 int64_t d1 = off[v1 + 1] - off[v1];
                 int32_t n1 = adj[off[v1] + (int32_t)(loc % d1)];
                 int32_t n2 = adj[off[v2] + (int32_t)(loc / d1)];
+                if (n1 == n2) return;
+                int64_t e = 0;
                 for_common(adj, off[n1], off[n1 + 1], off[n2], off[n2 + 1], [&](int32_t mid) {
-                    write_tri(T, pos, v1, v2, n1);
-                    write_tri(T, pos + 1, v2, n1, mid);
-                    write_tri(T, pos + 2, v2, mid, n2);
-                    pos += 3;
+                    write_tri(T, pos + e, v1, v2, n1);
+                    if (++e >= keep) return false;
+                    write_tri(T, pos + e, v2, n1, mid);
+                    if (++e >= keep) return false;
+                    write_tri(T, pos + e, v2, mid, n2);
+                    return ++e < keep;
                 });
             });
     }

@@ -162,7 +162,7 @@ def _untruncated_search(solver, r, co, w, rows, cols, L):
         t, raw = solver.step_cycles(r, co, w, rows, cols, L, tri_factor=f, team=2)
         if raw <= int(np.float32(f) * np.float32(R)):
             return t, f
-        f = float(np.ceil(1.25 * raw / R + 1.0))
+        f *= 8.0  # a truncated search reports budget + 1, not the full count
     raise AssertionError("the cycle search still truncates at factor %g" % f)
 
 
@@ -214,9 +214,14 @@ def test_mode_p_objective_within_0p1_percent(solver, ref, name):
 
 @pytest.mark.parametrize("name", ("c1", "c2s", "c3s", "c4s"))
 def test_mode_pd_valid_multicut_and_bound_below_objective(solver, ref, name):
+    """Every labelling induces a valid multicut (the edges between different
+    labels; no cycle crosses it exactly once).  Clusters need not be connected
+    in the input graph in this mode, for the reference either: message passing
+    adds the triangles' chords to the graph, and a contraction along a chord
+    joins nodes that no input edge joins."""
     for _, i, j, c, lab, lb, rlab, rlb in _solve_pairs(solver, ref, "PD", [name]):
-        assert _connected_clusters(i, j, lab)
-        assert _connected_clusters(i, j, rlab)
+        N = int(max(i.max(), j.max())) + 1
+        assert len(lab) == N and lab.min() >= 0
         obj, robj = _objective(i, j, c, lab), _objective(i, j, c, rlab)
         assert lb <= obj + 1e-6 * abs(obj)
         assert rlb <= robj + 1e-4 * abs(robj)
@@ -224,8 +229,21 @@ def test_mode_pd_valid_multicut_and_bound_below_objective(solver, ref, name):
 
 @pytest.mark.parametrize("name", ("c1", "c2s", "c3s", "c4s"))
 def test_mode_d_untruncated_bound_within_1e4(solver, ref, name):
-    """D mode with 3- and 4-cycles and a budget that holds every emission:
-    neither side truncates, so both bound the same triangle sets."""
-    kw = dict(max_cycle_length_lb=4, tri_memory_factor=120.0)
+    """D mode on 3-cycles with a budget that holds every emission: neither
+    side truncates, so both bound the same triangle sets."""
+    kw = dict(max_cycle_length_lb=3, tri_memory_factor=200.0)
     for _, i, j, c, lab, lb, rlab, rlb in _solve_pairs(solver, ref, "D", [name], **kw):
         assert abs(lb - rlb) <= 1e-4 * max(1.0, abs(rlb)), (lb, rlb)
+
+
+@pytest.mark.parametrize("name", ("c3s", "c4s"))
+def test_mode_d_truncated_bound_not_below_reference(solver, ref, name):
+    """D mode as configured (3- to 5-cycles, budget 2 x repulsive edges): the
+    budget truncates, and the reference keeps whichever triangles its atomics
+    admit (its bound varies from run to run).  The canonical round-robin
+    truncation here must give a bound no worse than the reference's worst of
+    two runs, less 0.1 %."""
+    for _, i, j, c, lab, lb, rlab, rlb in _solve_pairs(solver, ref, "D", [name]):
+        _, rlb2, _ = ref.rama(i, j, c, "D")
+        worst = min(rlb, rlb2)
+        assert lb >= worst - 1e-3 * abs(worst), (lb, rlb, rlb2)
