@@ -251,7 +251,10 @@ __device__ void conflicted_cycles(const Team &t, Scratch &sc, char *sm, const Gr
     tb.budget = 0;
     tb.t1 = tb.t2 = tb.t3 = nullptr;
     if (max_len < 3 || A.n == 0) return;
-    const float mn = team_min<Team, float>(t, sc, sm, A.n, 3.4e38f, [&](int64_t e) { return A.cost[e]; });
+    // the smallest cost: known from the pass that built the graph, or one pass
+    const float mn = A.cmin == A.cmin
+                         ? A.cmin
+                         : team_min<Team, float>(t, sc, sm, A.n, 3.4e38f, [&](int64_t e) { return A.cost[e]; });
     const float thresh = mn * tol;          // determine_threshold (:170-174)
     const float pos_tol = -1.0f * thresh;   // create_matrices (:176-220)
     const int32_t N = A.max_dim();
@@ -271,23 +274,23 @@ __device__ void conflicted_cycles(const Team &t, Scratch &sc, char *sm, const Gr
         haspos[A.col[e]] = 1;
         return 1;
     });
-    // one scan counts both: the low 32 bits count every repulsive edge (the
-    // budget counts them all, :247), the high bits the kept ones
-    const int64_t packed = team_scan<Team, int64_t>(
-        t, sc, sm, A.n,
-        [&](int64_t e) -> int64_t {
-            if (!(A.cost[e] < thresh)) return 0;
-            return (haspos[A.row[e]] && haspos[A.col[e]]) ? (int64_t(1) << 32) + 1 : 1;
-        },
-        [&](int64_t e, int64_t pre, int64_t v) {
-            if (v >> 32) ridx[pre >> 32] = e;
-        });
+    // one pass counts both: the low 32 bits count every repulsive edge (the
+    // budget counts them all, :247), the high bits the kept ones; the kept
+    // ones are compacted only when there are any
+    auto rep_code = [&](int64_t e) -> int64_t {
+        if (!(A.cost[e] < thresh)) return 0;
+        return (haspos[A.row[e]] && haspos[A.col[e]]) ? (int64_t(1) << 32) + 1 : 1;
+    };
+    const int64_t packed = team_sum<Team, int64_t>(t, sc, sm, A.n, rep_code);
     const int64_t Rall = packed & 0xffffffffll;
     const int64_t R = packed >> 32;
-    if (P == 0 || R == 0) {
-        sc.alg_bytes += 12.0 * (double)A.n;
-        return;
-    }
+    sc.alg_bytes += 12.0 * (double)A.n;
+    if (P == 0 || R == 0) return;
+    team_scan<Team, int64_t>(
+        t, sc, sm, A.n, [&](int64_t e) -> int64_t { return rep_code(e) >> 32; },
+        [&](int64_t e, int64_t pre, int64_t v) {
+            if (v) ridx[pre] = e;
+        });
     Csr C = build_symmetric_csr(t, sc, sm, A, N, [&](int64_t e) { return A.cost[e] > pos_tol; }, false);
     const int64_t budget = (int64_t)(int32_t)(tri_factor * (float)Rall);  // (:247)
     tb.budget = budget < 0 ? 0 : budget;
@@ -387,7 +390,7 @@ __device__ void conflicted_cycles(const Team &t, Scratch &sc, char *sm, const Gr
             });
     }
     tb.num = tb.count < tb.budget ? tb.count : tb.budget;
-    sc.alg_bytes += 12.0 * (double)A.n + 8.0 * (double)R + 4.0 * (double)C.m2 + 12.0 * (double)tb.num;
+    sc.alg_bytes += 8.0 * (double)R + 4.0 * (double)C.m2 + 12.0 * (double)tb.num;
 }
 
 }  // namespace rama

@@ -12,8 +12,11 @@ struct Graph {
     float *cost;
     int64_t n;
     int32_t rows, cols;  // dCOO::rows_ / cols_
+    float cmin;          // smallest cost of an edge with row != col (NaN: not known)
     __device__ __forceinline__ int32_t max_dim() const { return rows > cols ? rows : cols; }
 };
+
+__device__ __forceinline__ float unknown_cost() { return __int_as_float(0x7fc00000); }
 
 // Scratch arrays of a new graph, allocated in the temporaries.
 template <class Team>
@@ -25,6 +28,7 @@ __device__ Graph graph_alloc(const Team &t, Scratch &sc, int64_t n)
     g.cost = sc.arena.take<float>(n + 1);
     g.n = n;
     g.rows = g.cols = 0;
+    g.cmin = unknown_cost();
     return g;
 }
 
@@ -57,17 +61,25 @@ __device__ Graph graph_commit(const Team &t, Scratch &sc, const Graph &src)
 }
 
 // dims as in dCOO::init (src/dCOO.cu:47-51): rows = last row + 1,
-// cols = max col + 1 (0 for an empty graph)
+// cols = max col + 1 (0 for an empty graph); in the same pass, the smallest
+// cost of an edge that is not a self-loop (dCOO::min of the graph once its
+// diagonal is removed; the cycle search's threshold, src/conflicted_cycles_cuda.cu:170-174)
 template <class Team>
 __device__ void graph_set_dims(const Team &t, Scratch &sc, char *sm, Graph &g)
 {
     if (g.n == 0) {
         g.rows = g.cols = 0;
+        g.cmin = unknown_cost();
         return;
     }
-    int32_t mc = team_max<Team, int32_t>(t, sc, sm, g.n, -1, [&](int64_t e) { return g.col[e]; });
+    int32_t mc = -1;
+    float mn = 3.4e38f;
+    team_maxi_minf(
+        t, sc, sm, g.n, -1, 3.4e38f, [&](int64_t e) { return g.col[e]; },
+        [&](int64_t e) { return g.row[e] != g.col[e] ? g.cost[e] : 3.4e38f; }, mc, mn);
     g.cols = mc + 1;
     g.rows = uread(&g.row[g.n - 1]) + 1;
+    g.cmin = mn;
 }
 
 __device__ __forceinline__ uint64_t pack_key(int32_t a, int32_t b, int nbits)
@@ -192,8 +204,8 @@ __device__ void contract_sorted_keys(const Team &t, Scratch &sc, char *sm, const
 }
 
 template <class Team>
-__device__ Graph graph_contract(const Team &t, Scratch &sc, char *sm, const Graph &A, const int32_t *map,
-                                int32_t map_max, int *bad)
+__device__ Graph graph_contract_sorted(const Team &t, Scratch &sc, char *sm, const Graph &A, const int32_t *map,
+                                       int32_t map_max, int *bad)
 {
     const int64_t n = A.n;
     const int nb = bits_for((uint64_t)(map_max > 0 ? map_max : 0));
@@ -258,10 +270,172 @@ __device__ Graph graph_contract(const Team &t, Scratch &sc, char *sm, const Grap
     h.n = nk;
     h.rows = g.rows;
     h.cols = g.cols;
+    h.cmin = g.cmin;
     Graph res = graph_commit(t, sc, h);
     sc.arena.release(m);
     sc.alg_bytes += 20.0 * (double)n + 12.0 * (double)nruns;
     return res;
+}
+
+// The contraction (dCOO::contract_cuda + has_bad_contractions +
+// remove_diagonal) by buckets of the new row:
+//   1. each edge's contracted endpoints (lo, hi) are computed once, with its
+//      slot in bucket lo;
+//   2. the bucket sort orders every bucket by (hi, edge index) and carries the
+//      edge's cost bits along (no gather afterwards);
+//   3. one thread per bucket walks its runs of equal hi: RSUM of a run's
+//      costs in edge order (runs of more than 32 by a warp afterwards), the
+//      diagonal run's sum checked for a bad contraction, the others written
+//      back into the bucket's own range; the largest hi and the last
+//      non-empty bucket give the dims (taken before the diagonal goes, as the
+//      reference does);
+//   4. a scan of the per-bucket counts places the rows, and the edges are
+//      written straight into the graph slot at the top of the arena (the old
+//      graph there is dead by then), with the smallest cost for the cycle
+//      search.
+// A bucket of more than BUCKET_MAX edges sends the contraction to
+// graph_contract_sorted (one radix sort of the packed keys).  Both give the
+// same graph bit for bit.
+template <class Team>
+__device__ Graph graph_contract(const Team &t, Scratch &sc, char *sm, const Graph &A, const int32_t *map,
+                                int32_t map_max, int *bad)
+{
+    const int64_t n = A.n;
+    Graph out = A;
+    if (n >= (int64_t(1) << 31)) return graph_contract_sorted(t, sc, sm, A, map, map_max, bad);
+    const int32_t nbk = map_max + 1;
+    uint64_t m = sc.arena.mark();
+    int2 *lohi = sc.arena.take<int2>(n + 1);
+    uint64_t *sk = sc.arena.take<uint64_t>(n + 1);
+    int32_t *sbits = sc.arena.take<int32_t>(n + 1);
+    int32_t *bst = sc.arena.take<int32_t>((int64_t)nbk + 2);
+    int32_t *cnt = sc.arena.take<int32_t>((int64_t)nbk + 2);
+    int32_t *opos = sc.arena.take<int32_t>((int64_t)nbk + 2);
+    int32_t *rcol = sc.arena.take<int32_t>(n + 1);
+    float *rcost = sc.arena.take<float>(n + 1);
+    int4 *longq = sc.arena.take<int4>(n / 33 + 2);
+    // [0] bad, [1] long runs, [2] max hi, [3] last non-empty bucket, [4] smallest cost (ordered bits)
+    int32_t *fl = sc.arena.take<int32_t>(8);
+    if (!sc.arena.ok()) return out;
+    if (t.rank() == 0) {
+        fl[0] = 0;
+        fl[1] = 0;
+        fl[2] = -1;
+        fl[3] = -1;
+        fl[4] = (int32_t)0xffffffffu;
+    }
+    const bool done = team_bucket_sort_ex(
+        t, sc, sm, n, nbk,
+        [&](int64_t e) {
+            const int32_t a = map[A.row[e]], b = map[A.col[e]];
+            const int32_t lo = a < b ? a : b, hi = a < b ? b : a;
+            lohi[e] = make_int2(lo, hi);
+            return lo;
+        },
+        [&](int64_t e) { return lohi[e].x; },
+        [&](int64_t e) -> uint64_t { return ((uint64_t)(uint32_t)lohi[e].y << 32) | (uint64_t)e; },
+        [&](int64_t e) { return __float_as_int(A.cost[e]); }, sk, sbits, bst);
+    if (!done) {
+        sc.arena.release(m);
+        return graph_contract_sorted(t, sc, sm, A, map, map_max, bad);
+    }
+    // 3. runs of every bucket
+    int32_t mxhi = -1, lastb = -1;
+    for (int64_t b = t.rank(); b < nbk; b += t.size()) {
+        const int32_t s = bst[b], e = bst[b + 1];
+        int32_t k = 0;
+        for (int32_t p = s; p < e;) {
+            const int32_t hi = (int32_t)(sk[p] >> 32);
+            int32_t q = p + 1;
+            while (q < e && (int32_t)(sk[q] >> 32) == hi) ++q;
+            mxhi = hi > mxhi ? hi : mxhi;
+            const bool diag = hi == (int32_t)b;
+            if (q - p <= 32) {
+                const float v = rsum_serial(q - p, [&](int x) { return __int_as_float(sbits[p + x]); });
+                if (diag) {
+                    if (v < 0.0f) fl[0] = 1;
+                } else {
+                    rcol[s + k] = hi;
+                    rcost[s + k] = v;
+                }
+            } else {
+                const int32_t slot = atomicAdd(&fl[1], 1);
+                longq[slot] = make_int4(p, q, diag ? -1 : s + k, 0);
+                if (!diag) rcol[s + k] = hi;
+            }
+            if (!diag) ++k;
+            p = q;
+        }
+        cnt[b] = k;
+        if (e > s) lastb = (int32_t)b;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        mxhi = max(mxhi, __shfl_xor_sync(FULL, mxhi, o));
+        lastb = max(lastb, __shfl_xor_sync(FULL, lastb, o));
+    }
+    if (lane_id() == 0) {
+        if (mxhi >= 0) atomicMax(&fl[2], mxhi);
+        if (lastb >= 0) atomicMax(&fl[3], lastb);
+    }
+    t.sync();
+    const int32_t nl = uread(&fl[1]);
+    for (int64_t w = team_warp(t); w < nl; w += team_nwarps(t)) {
+        const int4 L = longq[w];
+        const float v = rsum_warp(L.y - L.x, [&](int64_t x) { return __int_as_float(sbits[L.x + x]); });
+        if (lane_id() == 0) {
+            if (L.z < 0) {
+                if (v < 0.0f) fl[0] = 1;
+            } else {
+                rcost[L.z] = v;
+            }
+        }
+    }
+    // 4. rows placed by a scan of the counts, edges written into the slot
+    const int64_t nk = team_scan<Team, int64_t>(
+        t, sc, sm, nbk, [&](int64_t b) -> int64_t { return cnt[b]; },
+        [&](int64_t b, int64_t pre, int64_t) { opos[b] = (int32_t)pre; });
+    *bad = uread(&fl[0]);
+    Arena &ar = sc.arena;
+    const uint64_t bytes = (uint64_t)(nk + 1) * 12 + 3 * 256;
+    const uint64_t top = (ar.cap - bytes) & ~uint64_t(255);
+    if (ar.failed || bytes > ar.cap || top < ar.lo) {
+        ar.failed = 1;
+        return out;
+    }
+    const uint64_t words = ((uint64_t)(nk + 1) * 4 + 255) / 256 * 256;
+    Graph h;
+    h.row = reinterpret_cast<int32_t *>(ar.base + top);
+    h.col = reinterpret_cast<int32_t *>(ar.base + top + words);
+    h.cost = reinterpret_cast<float *>(ar.base + top + 2 * words);
+    h.n = nk;
+    h.rows = uread(&fl[3]) + 1;
+    h.cols = uread(&fl[2]) + 1;
+    uint32_t mn = 0xffffffffu;
+    for (int64_t b = t.rank(); b < nbk; b += t.size()) {
+        const int32_t s = bst[b], o = opos[b], c = cnt[b];
+        for (int32_t k = 0; k < c; ++k) {
+            const float v = rcost[s + k];
+            h.row[o + k] = (int32_t)b;
+            h.col[o + k] = rcol[s + k];
+            h.cost[o + k] = v;
+            const uint32_t f = float_ordered(v);
+            mn = f < mn ? f : mn;
+        }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const uint32_t x = __shfl_xor_sync(FULL, mn, o);
+        mn = x < mn ? x : mn;
+    }
+    if (lane_id() == 0 && mn != 0xffffffffu) atomicMin(reinterpret_cast<unsigned *>(&fl[4]), mn);
+    t.sync();
+    const uint32_t mo = (uint32_t)uread(&fl[4]);
+    h.cmin = nk > 0 ? __uint_as_float((mo & 0x80000000u) ? (mo & 0x7fffffffu) : ~mo) : unknown_cost();
+    ar.top = top;
+    sc.arena.release(m);
+    sc.alg_bytes += 20.0 * (double)n + 12.0 * (double)nk;
+    return h;
 }
 
 // compute_sanitized_graph (include/rama_utils.h:429-466): drop duplicate

@@ -16,6 +16,15 @@ namespace rama {
 // complemented neighbour id), which gives the same choice without building
 // the CSR.  The offers of one iteration go to one of two key arrays; the
 // match pass reads it and clears the other for the next iteration.
+//
+// Only edges above the threshold between two unmatched vertices can offer:
+// the first iteration reads every edge and appends those to a candidate list,
+// and each later iteration reads the list and appends its still-unmatched
+// edges to the next one.  The vertices that received an offer go to a
+// touched list, and only they are matched, cleared and counted.  Lists are
+// appended with warp-aggregated atomics, so their order varies, but an
+// atomicMax and the per-vertex match do not depend on the order: the map is
+// the same as with full passes.
 template <class Team>
 __device__ int32_t matching_contraction_map(const Team &t, Scratch &sc, char *sm, const Graph &A, float mm,
                                             int32_t *map_out, int32_t *M_out)
@@ -29,7 +38,7 @@ __device__ int32_t matching_contraction_map(const Team &t, Scratch &sc, char *sm
     unsigned long long *offer[2];
     offer[0] = sc.arena.take<unsigned long long>((int64_t)M + 1);
     offer[1] = sc.arena.take<unsigned long long>((int64_t)M + 1);
-    int32_t *flags = sc.arena.take<int32_t>(16);
+    int32_t *flags = sc.arena.take<int32_t>(64);  // [it]: matched a pair; [16 + 2k]: list sizes
     if (!sc.arena.ok()) return 0;
     for (int64_t v = t.rank(); v < M; v += t.size()) {
         nm[v] = (int32_t)v;
@@ -37,7 +46,7 @@ __device__ int32_t matching_contraction_map(const Team &t, Scratch &sc, char *sm
         offer[0][v] = 0ull;
         offer[1][v] = 0ull;
     }
-    if (t.rank() < 16) flags[t.rank()] = 0;
+    if (t.rank() < 64) flags[t.rank()] = 0;
     // determine_matching_threshold (:76-86): mean of the non-negative costs
     // of the doubled edge list, CSUM over the directed list
     const double S = team_csum(t, sc, A.n, [&](int64_t e) -> double {
@@ -49,46 +58,120 @@ __device__ int32_t matching_contraction_map(const Team &t, Scratch &sc, char *sm
     if (K > 0) {
         const float sum_f = (float)(2.0 * S);
         const float thresh = (mm * sum_f) / (float)(2 * K);
+        // candidate edges (u, v, order-preserving cost bits), two lists
+        uint64_t lm = sc.arena.mark();
+        const int64_t cap = A.n + 1;
+        int2 *cand[2];
+        uint32_t *cbits[2];
+        cand[0] = sc.arena.take<int2>(cap);
+        cand[1] = sc.arena.take<int2>(cap);
+        cbits[0] = sc.arena.take<uint32_t>(cap);
+        cbits[1] = sc.arena.take<uint32_t>(cap);
+        int32_t *touched[2];
+        touched[0] = sc.arena.take<int32_t>((int64_t)M + 1);
+        touched[1] = sc.arena.take<int32_t>((int64_t)M + 1);
+        if (!sc.arena.ok()) {
+            sc.arena.release(mark);
+            return 0;
+        }
+        int64_t ncand = 0;      // entries of the list read by this iteration
+        int32_t ntouch_prev = 0;  // vertices touched by the previous iteration
         for (int it = 0; it < 10; ++it) {
-            unsigned long long *cur_offer = offer[it & 1], *next_offer = offer[(it + 1) & 1];
-            // pick_best_neighbour: every edge above the threshold between two
-            // unmatched vertices offers itself to both
-            for (int64_t e = t.rank(); e < A.n; e += t.size()) {
-                const float c = A.cost[e];
-                if (!(c > thresh)) continue;
-                const int32_t u = A.row[e], v = A.col[e];
-                if (u == v || matched[u] || matched[v]) continue;
-                const unsigned long long hi = (unsigned long long)float_ordered(c) << 32;
-                atomicMax(&cur_offer[u], hi | (unsigned long long)(~(uint32_t)v));
-                atomicMax(&cur_offer[v], hi | (unsigned long long)(~(uint32_t)u));
+            const int cur = it & 1, nxt = cur ^ 1;
+            unsigned long long *cur_offer = offer[cur], *next_offer = offer[nxt];
+            int32_t *cnt_next = flags + 16 + 2 * (it & 7);  // [0]: next list, [1]: touched
+            int32_t *cnt_clear = flags + 16 + 2 * ((it + 1) & 7);
+            // pick_best_neighbour: every live candidate offers itself to both
+            // ends; it stays a candidate for the next iteration
+            auto offer_edge = [&](int32_t u, int32_t v, uint32_t hb, bool live) {
+                unsigned long long ou = 0, ov = 0;
+                if (live) {
+                    const unsigned long long hi = (unsigned long long)hb << 32;
+                    ou = atomicMax(&cur_offer[u], hi | (unsigned long long)(~(uint32_t)v));
+                    ov = atomicMax(&cur_offer[v], hi | (unsigned long long)(~(uint32_t)u));
+                }
+                // append the edge to the next list and first-touched vertices
+                // to the touched list (one atomic per warp for each)
+                const unsigned bl = __ballot_sync(FULL, live);
+                int32_t base = 0;
+                if (lane_id() == 0 && bl) base = atomicAdd(&cnt_next[0], __popc(bl));
+                base = __shfl_sync(FULL, base, 0);
+                if (live) {
+                    const int32_t p = base + __popc(bl & lanemask_lt());
+                    cand[nxt][p] = make_int2(u, v);
+                    cbits[nxt][p] = hb;
+                }
+                const bool fu = live && ou == 0ull, fv = live && ov == 0ull;
+                const unsigned bu = __ballot_sync(FULL, fu), bv = __ballot_sync(FULL, fv);
+                int32_t tb = 0;
+                if (lane_id() == 0 && (bu | bv)) tb = atomicAdd(&cnt_next[1], __popc(bu) + __popc(bv));
+                tb = __shfl_sync(FULL, tb, 0);
+                if (fu) touched[cur][tb + __popc(bu & lanemask_lt())] = u;
+                if (fv) touched[cur][tb + __popc(bu) + __popc(bv & lanemask_lt())] = v;
+            };
+            if (it == 0) {
+                for (int64_t base = (int64_t)t.rank() - lane_id(); base < A.n; base += t.size()) {
+                    const int64_t e = base + lane_id();
+                    const float c = e < A.n ? A.cost[e] : 0.0f;
+                    const bool live = e < A.n && c > thresh && A.row[e] != A.col[e];
+                    offer_edge(live ? A.row[e] : 0, live ? A.col[e] : 0, float_ordered(c), live);
+                }
+            } else {
+                const int2 *L = cand[cur];
+                const uint32_t *LB = cbits[cur];
+                for (int64_t base = (int64_t)t.rank() - lane_id(); base < ncand; base += t.size()) {
+                    const int64_t q = base + lane_id();
+                    int2 uv = make_int2(0, 0);
+                    uint32_t hb = 0;
+                    bool live = false;
+                    if (q < ncand) {
+                        uv = L[q];
+                        hb = LB[q];
+                        live = !matched[uv.x] && !matched[uv.y];
+                    }
+                    offer_edge(uv.x, uv.y, hb, live);
+                }
             }
+            if (t.rank() < 2) cnt_clear[t.rank()] = 0;  // counters of the iteration after next
             t.sync();
-            // match_neighbours (:49-74): mutual best offers pair up
-            for (int64_t v = t.rank(); v < M; v += t.size()) {
-                next_offer[v] = 0ull;
-                if (matched[v]) continue;
+            const int64_t nread = it == 0 ? A.n : ncand;
+            const int32_t ntouch = uread(&cnt_next[1]);
+            ncand = uread(&cnt_next[0]);
+            // match_neighbours (:49-74): mutual best offers pair up; the other
+            // offer buffer is cleared where the previous iteration wrote it
+            const int32_t *T0 = touched[cur];
+            const int32_t *Tp = touched[nxt];
+            for (int64_t k = t.rank(); k < ntouch_prev; k += t.size()) next_offer[Tp[k]] = 0ull;
+            for (int64_t k = t.rank(); k < ntouch; k += t.size()) {
+                const int32_t v = T0[k];
                 const unsigned long long o = cur_offer[v];
-                if (!o) continue;
                 const int32_t b = (int32_t)(~(uint32_t)(o & 0xffffffffull));
                 const unsigned long long ob = cur_offer[b];
-                if (ob && (int32_t)(~(uint32_t)(ob & 0xffffffffull)) == (int32_t)v) {
-                    if ((int32_t)v < b) {
-                        nm[b] = (int32_t)v;
-                        matched[v] = 1;
-                        matched[b] = 1;
-                        flags[it] = 1;
-                    }
+                if (ob && (int32_t)(~(uint32_t)(ob & 0xffffffffull)) == v && v < b) {
+                    nm[b] = v;
+                    matched[v] = 1;
+                    matched[b] = 1;
+                    flags[it] = 1;
                 }
             }
             t.sync();
-            sc.alg_bytes += 20.0 * (double)A.n + 24.0 * (double)M;
-            int32_t cur = team_sum<Team, int32_t>(t, sc, sm, M, [&](int64_t v) { return matched[v]; });
-            float rel = (float)(cur - prev) / ((float)prev + 1.0f);
-            prev = cur;
+            sc.alg_bytes += 12.0 * (double)nread + 24.0 * (double)ntouch;
+            // new pairs, each counted at its smaller end v: the only touched
+            // vertex that is matched and whose best offer b was mapped to it
+            const int32_t pairs = team_sum<Team, int32_t>(t, sc, sm, ntouch, [&](int64_t k) -> int32_t {
+                const int32_t v = T0[k];
+                const int32_t b = (int32_t)(~(uint32_t)(cur_offer[v] & 0xffffffffull));
+                return matched[v] && nm[b] == v ? 1 : 0;
+            });
+            const int32_t curm = prev + 2 * pairs;
+            float rel = (float)(curm - prev) / ((float)prev + 1.0f);
+            prev = curm;
+            ntouch_prev = ntouch;
             if (!uread(&flags[it]) || (double)rel < 0.1) break;
-            // vertices matched in this iteration must not take offers of the
-            // next one: the offer pass reads `matched` after this sync
+            // vertices matched in this iteration take no offers in the next:
+            // the next offer pass reads `matched` after this sync
         }
+        sc.arena.release(lm);
     }
     compress_labels(t, sc, sm, nm, M, M - 1, map_out);
     sc.arena.release(mark);

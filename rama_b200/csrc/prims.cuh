@@ -256,11 +256,77 @@ __device__ T team_min(const Team &t, Scratch &sc, char *sm, int64_t n, T init, G
     return warp_fold_parts<T>(part, t.nblocks(), init, [](T a, T b) { return b < a ? b : a; });
 }
 
+// The maximum of ia(i) and the minimum of fb(i) over [0, n) in one pass and
+// one team sync (both exact, so the result does not depend on the order).
+template <class Team, class IA, class FB>
+__device__ void team_maxi_minf(const Team &t, Scratch &sc, char *sm, int64_t n, int32_t iinit, float finit, IA ia,
+                               FB fb, int32_t &imax, float &fmin)
+{
+    int32_t a = iinit;
+    float b = finit;
+    for (int64_t i = t.rank(); i < n; i += t.size()) {
+        const int32_t x = ia(i);
+        const float y = fb(i);
+        a = x > a ? x : a;
+        b = y < b ? y : b;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const int32_t x = __shfl_xor_sync(FULL, a, o);
+        const float y = __shfl_xor_sync(FULL, b, o);
+        a = x > a ? x : a;
+        b = y < b ? y : b;
+    }
+    int32_t *sa = reinterpret_cast<int32_t *>(sm);
+    float *sb = reinterpret_cast<float *>(sm + 128);
+    if (lane_id() == 0) {
+        sa[warp_in_block()] = a;
+        sb[warp_in_block()] = b;
+    }
+    __syncthreads();
+    a = sa[0];
+    b = sb[0];
+    for (int k = 1; k < (int)(blockDim.x >> 5); ++k) {
+        a = sa[k] > a ? sa[k] : a;
+        b = sb[k] < b ? sb[k] : b;
+    }
+    __syncthreads();
+    int32_t *part = reinterpret_cast<int32_t *>(sc.next_part());  // 16 B per block
+    if (threadIdx.x == 0) {
+        part[2 * t.block()] = a;
+        part[2 * t.block() + 1] = __float_as_int(b);
+    }
+    t.sync();
+    a = iinit;
+    b = finit;
+    for (int k = lane_id(); k < t.nblocks(); k += 32) {
+        const int32_t x = __ldcg(part + 2 * k);
+        const float y = __int_as_float(__ldcg(part + 2 * k + 1));
+        a = x > a ? x : a;
+        b = y < b ? y : b;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const int32_t x = __shfl_xor_sync(FULL, a, o);
+        const float y = __shfl_xor_sync(FULL, b, o);
+        a = x > a ? x : a;
+        b = y < b ? y : b;
+    }
+    imax = a;
+    fmin = b;
+}
+
 // ---------------------------------------------------------------------------
 // team exclusive scan: out(i, prefix, value) is called for every i in [0,n)
 // in chunk order; returns the total.  Two team syncs; outputs are visible to
-// the whole team on return.
+// the whole team on return.  The second pass takes tiles of SCAN_ITEMS
+// consecutive elements per thread: a serial scan in registers and one block
+// scan per tile (one block scan per SCAN_ITEMS x blockDim elements keeps the
+// CTA's barriers few).  Integer sums only, so the result does not depend on
+// the tiling.
 // ---------------------------------------------------------------------------
+constexpr int SCAN_ITEMS = 8;
+
 template <class Team, class T, class In, class Out>
 __device__ T team_scan(const Team &t, Scratch &sc, char *sm, int64_t n, In in, Out out)
 {
@@ -281,12 +347,23 @@ __device__ T team_scan(const Team &t, Scratch &sc, char *sm, int64_t n, In in, O
     }
     base = warp_sum(base);
     total = warp_sum(total);
-    for (int64_t tile = lo; tile < hi; tile += blockDim.x) {
-        int64_t i = tile + threadIdx.x;
-        T v = i < hi ? in(i) : T(0);
+    const int64_t TILE = (int64_t)blockDim.x * SCAN_ITEMS;
+    for (int64_t tile = lo; tile < hi; tile += TILE) {
+        const int64_t i0 = tile + (int64_t)threadIdx.x * SCAN_ITEMS;
+        T v[SCAN_ITEMS];
+        T mine = T(0);
+#pragma unroll
+        for (int k = 0; k < SCAN_ITEMS; ++k) {
+            v[k] = i0 + k < hi ? in(i0 + k) : T(0);
+            mine += v[k];
+        }
         T ts;
-        T ex = block_excl_scan<T>(v, tsm, ts);
-        if (i < hi) out(i, base + ex, v);
+        T run = base + block_excl_scan<T>(mine, tsm, ts);
+#pragma unroll
+        for (int k = 0; k < SCAN_ITEMS; ++k) {
+            if (i0 + k < hi) out(i0 + k, run, v[k]);
+            run += v[k];
+        }
         base += ts;
     }
     t.sync();
@@ -779,9 +856,14 @@ __device__ __forceinline__ void smem_bitonic(uint64_t *key, int32_t *idx, int m,
     }
 }
 
-template <class Team, class Bk, class Sub>
-__device__ bool team_bucket_sort(const Team &t, Scratch &sc, char *sm, int64_t n, int32_t nb, Bk bucket, Sub sub,
-                                 uint64_t *keys_out, int32_t *idx_out, int32_t *bstart)
+// The general form: the slot pass calls bk_slot(i) once per item (it may
+// store what it computes for the scatter pass), the scatter pass calls
+// bucket(i), sub(i) and pay(i); idx_out receives pay(i) of each item instead of
+// its index (team_bucket_sort below: pay(i) = i).
+template <class Team, class BkSlot, class Bk, class Sub, class Pay>
+__device__ bool team_bucket_sort_ex(const Team &t, Scratch &sc, char *sm, int64_t n, int32_t nb, BkSlot bk_slot,
+                                    Bk bucket, Sub sub, Pay pay, uint64_t *keys_out, int32_t *idx_out,
+                                    int32_t *bstart)
 {
     uint64_t am = sc.arena.mark();
     int32_t *slot = sc.arena.take<int32_t>(n + 1);
@@ -799,7 +881,7 @@ __device__ bool team_bucket_sort(const Team &t, Scratch &sc, char *sm, int64_t n
     for (int64_t base = (int64_t)t.rank() - lane_id(); base < n; base += t.size()) {
         const int64_t i = base + lane_id();
         const bool valid = i < n;
-        const int32_t b = valid ? (int32_t)bucket(i) : -1;
+        const int32_t b = valid ? (int32_t)bk_slot(i) : -1;
         const unsigned peers = __match_any_sync(FULL, b);
         const int leader = __ffs(peers) - 1;
         int32_t s0 = 0;
@@ -830,7 +912,7 @@ __device__ bool team_bucket_sort(const Team &t, Scratch &sc, char *sm, int64_t n
         const int32_t b = (int32_t)bucket(i);
         const int64_t p = (int64_t)bstart[b] + slot[i];
         tk[p] = sub(i);
-        ti[p] = (int32_t)i;
+        ti[p] = pay(i);
         tb[p] = b;
     }
     t.sync();
@@ -906,6 +988,14 @@ __device__ bool team_bucket_sort(const Team &t, Scratch &sc, char *sm, int64_t n
     t.sync();
     sc.arena.release(am);
     return true;
+}
+
+template <class Team, class Bk, class Sub>
+__device__ bool team_bucket_sort(const Team &t, Scratch &sc, char *sm, int64_t n, int32_t nb, Bk bucket, Sub sub,
+                                 uint64_t *keys_out, int32_t *idx_out, int32_t *bstart)
+{
+    return team_bucket_sort_ex(
+        t, sc, sm, n, nb, bucket, bucket, sub, [](int64_t i) { return (int32_t)i; }, keys_out, idx_out, bstart);
 }
 
 // ---------------------------------------------------------------------------

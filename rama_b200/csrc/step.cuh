@@ -34,6 +34,7 @@ __device__ void run_step(const Team &t, char *sm, Scratch sc, rama_step_args *a)
     A.n = a->n;
     A.rows = a->rows;
     A.cols = a->cols;
+    A.cmin = unknown_cost();
     const int op = a->op;
     if (op == RAMA_STEP_INIT) {
         Graph g = graph_from_edges(t, sc, sm, a->i, a->j, a->c, a->m);

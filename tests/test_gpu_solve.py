@@ -15,7 +15,21 @@ def cases():
         out.append(("rnd%d" % s, instances.random_graph(n, deg, seed=100 + s)))
     out.append(("grid12", instances.grid2d(12, 12, seed=77)))
     out.append(("grid64", instances.grid2d(64, 64, seed=1001)))
+    out.append(("hub", hub_graph()))
     return out
+
+
+def hub_graph(spokes=6000, seed=5):
+    """Node 0 joined to `spokes` nodes, which form a ring: its row (and, after
+    a contraction, its cluster's row) holds more than 4096 edges, which sends
+    the bucket sorts of the initial sort and of the contraction to their radix
+    fallbacks."""
+    rng = np.random.default_rng(seed)
+    k = np.arange(1, spokes + 1, dtype=np.int32)
+    i = np.concatenate([np.zeros(spokes, np.int32), k[:-1]])
+    j = np.concatenate([k, k[1:]])
+    c = rng.normal(0.3, 1.0, size=len(i)).astype(np.float32)
+    return i, j, c
 
 
 CASES = cases()
