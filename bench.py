@@ -213,6 +213,7 @@ def run_ours(args, rank, world, local):
     N = int(max(i.max(), j.max())) + 1
     labels = torch.empty(N, dtype=torch.int32, device=dev)
     s = Solver(local)
+    tuning = tune_solver(s, local, args)
     stream = torch.cuda.current_stream(dev)
     st = C.c_void_p(stream.cuda_stream)
 
@@ -289,6 +290,7 @@ def run_ours(args, rank, world, local):
                      "traffic": traffic, "peak_source": src, "kernel": KERNEL_OF_TEAM.get(stats.team, "?"),
                      "kernel_ms": kms, "algorithmic_bytes": alg, "phases": phases},
         "clocks": clk.summary(),
+        "tuning": tuning,
     }
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(cfg, mode)
@@ -313,6 +315,20 @@ def phase_roofline(stats, hbm):
         gbs = b / (ms / 1e3) / 1e9 if ms > 0 else 0.0
         out[name] = {"ms": round(ms, 3), "bytes": b, "gbs": round(gbs, 1), "frac": round(gbs / hbm, 4)}
     return out
+
+
+def tune_solver(s, device, args):
+    """Launch parameters from the project's autotuner (rama_b200.autotune):
+    the cached choices for this device, tuned first when there are none.
+    None of them changes a result."""
+    if args.no_tune:
+        return {"source": "built-in defaults", "tuning": s.handle.tuning().as_dict()}
+    from rama_b200 import autotune
+
+    entry = autotune.ensure(device, budget_s=args.tune_budget)
+    autotune.apply(s.handle, device)
+    return {"source": entry["source"], "tuning": entry["tuning"], "default": entry["default"],
+            "tuning_s": entry.get("seconds")}
 
 
 def algorithmic_bytes(stats, E):
@@ -345,6 +361,7 @@ def run_ours_batch(args, rank, world, local):
     lo[1:] = np.cumsum(batch.node_counts)
     d_lab = torch.empty(int(lo[-1]), dtype=torch.int32, device=dev)
     s = Solver(local)
+    tuning = tune_solver(s, local, args)
     stream = torch.cuda.current_stream(dev)
     st = C.c_void_p(stream.cuda_stream)
     E = int(batch.edge_offsets[-1])
@@ -398,6 +415,7 @@ def run_ours_batch(args, rank, world, local):
                      "traffic": None, "peak_source": src, "kernel": "k_solve_cta", "kernel_ms": stats.device_ms,
                      "algorithmic_bytes": float(stats.alg_bytes)},
         "clocks": clk.summary(),
+        "tuning": tuning,
     }
 
 
@@ -686,6 +704,8 @@ def main():
     ap.add_argument("--lane-gb", type=int, default=8, help="c5: HBM budget per lane (GiB)")
     ap.add_argument("--plain-sample", type=int, default=200, help="c5: requests solved one at a time")
     ap.add_argument("--ref-sample", type=int, default=64, help="c4/c5 reference arm: instances timed")
+    ap.add_argument("--no-tune", action="store_true", help="keep the built-in launch parameters")
+    ap.add_argument("--tune-budget", type=float, default=45.0, help="seconds of autotuning trials when uncached")
     args = ap.parse_args()
     if args.config == "c5":
         # lanes overlap only when each stream has its own hardware queue

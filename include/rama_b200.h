@@ -87,9 +87,11 @@ typedef struct {
     double device_ms;        /* kernel time of the solve (CUDA events) */
     double alg_bytes;        /* algorithmic bytes of the solve: minimum edge, map, arc and triangle
                                 traffic of each phase, tallied on the device; no sort temporaries */
-    double phase_ms[10];     /* time per phase: init, cycle search, MP build, MP iterations + bound,
-                                dual commit, matching, forest contraction set, contraction, other, - */
-    double phase_bytes[10];  /* algorithmic bytes per phase (same order), the parts of alg_bytes */
+    double phase_ms[16];     /* time per phase: init, cycle search, MP build, MP iterations + bound,
+                                dual commit, matching (threshold, labels), forest contraction set,
+                                contraction (after its sort), other, matching iterations, contraction
+                                sort, CSR builds, then 4 unused */
+    double phase_bytes[16];  /* algorithmic bytes per phase (same order), the parts of alg_bytes */
 } rama_stats;
 
 /*
@@ -196,6 +198,25 @@ int rama_parse_multicut(rama_handle h, const char *d_text, int64_t len, int32_t 
  * to the device, parsed there, and the triples copied back). */
 int rama_parse_multicut_host(rama_handle h, const char *text, int64_t len, int32_t *i, int32_t *j, float *costs,
                              int64_t cap, int64_t *num_edges);
+
+/* Launch parameters of a handle.  None of them changes a result (every team
+ * computes the same solve, bit for bit); they only decide how the GPU's SMs
+ * are spent.  rama_create starts from built-in values;
+ * rama_b200/autotune.py measures better ones per device and sets them.  No
+ * counterpart in the reference (its launches have fixed shapes). */
+typedef struct {
+    int32_t grid_ctas_per_sm;    /* CTAs per SM of the whole-GPU solve (1 .. the occupancy maximum) */
+    int32_t cluster_ctas;        /* CTAs of a cluster team: 2, 4, 8 or 16 */
+    int64_t single_cluster_min;  /* a single solve of at least this many edges runs on a cluster ... */
+    int64_t single_grid_min;     /* ... and from this many on on the whole GPU (else on one CTA) */
+    int64_t batch_cluster_min;   /* batch instances below this size always run on one CTA; larger ones on */
+    float batch_cluster_share;   /* a cluster when they hold more than this many times the batch's edges
+                                    per CTA */
+} rama_tuning;
+int rama_get_tuning(rama_handle h, rama_tuning *out);
+/* RAMA_ERR_INVALID_ARG for a value outside its range or a cluster size that
+ * does not fit on the device. */
+int rama_set_tuning(rama_handle h, const rama_tuning *t);
 
 int rama_get_stats(rama_handle h, rama_stats *out);
 const char *rama_last_error(void);

@@ -56,11 +56,26 @@ class RamaStats(C.Structure):
         ("workspace_peak", C.c_int64),
         ("device_ms", C.c_double),
         ("alg_bytes", C.c_double),
-        ("phase_ms", C.c_double * 10),
-        ("phase_bytes", C.c_double * 10),
+        ("phase_ms", C.c_double * 16),
+        ("phase_bytes", C.c_double * 16),
     ]
 
-PHASES = ("init", "cycles", "mp_build", "mp_iter", "dual_commit", "matching", "woc", "contract", "other", "-")
+class RamaTuning(C.Structure):
+    _fields_ = [
+        ("grid_ctas_per_sm", C.c_int32),
+        ("cluster_ctas", C.c_int32),
+        ("single_cluster_min", C.c_int64),
+        ("single_grid_min", C.c_int64),
+        ("batch_cluster_min", C.c_int64),
+        ("batch_cluster_share", C.c_float),
+    ]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+PHASES = ("init", "cycles", "mp_build", "mp_iter", "dual_commit", "matching", "woc", "contract", "other",
+          "match_iter", "contract_sort", "csr", "-", "-", "-", "-")
 
 
 _P = C.c_void_p
@@ -90,7 +105,7 @@ class StepArgs(C.Structure):
 EXPORTS = ("rama_options_init", "rama_create", "rama_destroy", "rama_solve", "rama_solve_host", "rama_get_timeline",
            "rama_solve_batch", "rama_batch_launch", "rama_batch_poll", "rama_batch_wait", "rama_get_stats",
            "rama_last_error", "rama_objective", "rama_step", "rama_solve_small_static", "rama_parse_multicut",
-           "rama_parse_multicut_host")
+           "rama_parse_multicut_host", "rama_get_tuning", "rama_set_tuning")
 
 _lib = None
 _lock = threading.Lock()
@@ -133,6 +148,8 @@ def load():
         L.rama_last_error.restype = C.c_char_p
         L.rama_objective.argtypes = [P, P, P, P, i64, P, C.POINTER(C.c_double), P]
         L.rama_step.argtypes = [P, C.POINTER(StepArgs), P]
+        L.rama_get_tuning.argtypes = [P, C.POINTER(RamaTuning)]
+        L.rama_set_tuning.argtypes = [P, C.POINTER(RamaTuning)]
         _lib = L
         return L
 
@@ -179,6 +196,14 @@ class Handle:
             self.close()
         except Exception:
             pass
+
+    def tuning(self) -> RamaTuning:
+        t = RamaTuning()
+        check(load().rama_get_tuning(self.h, C.byref(t)))
+        return t
+
+    def set_tuning(self, t: RamaTuning):
+        check(load().rama_set_tuning(self.h, C.byref(t)))
 
     def stats(self) -> RamaStats:
         s = RamaStats()

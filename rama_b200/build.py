@@ -13,6 +13,7 @@ import glob
 import os
 import subprocess
 import sys
+import time
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
@@ -54,6 +55,9 @@ def build_lib(force=False, verbose=False):
     if not force and not _stale(LIB, units + headers) and all(os.path.exists(o) for o in objects):
         return LIB
     os.makedirs(objdir, exist_ok=True)
+    # Outputs are stamped with the time their compile started, so that a
+    # source edited while the build runs stays newer than its object.
+    started = time.time()
     procs, objs = [], []
     for u in units:
         o = os.path.join(objdir, os.path.basename(u)[:-3] + ".o")
@@ -63,11 +67,14 @@ def build_lib(force=False, verbose=False):
         cmd = [NVCC, *NVCC_FLAGS, "-c", "-o", o, u]
         if verbose:
             cmd.insert(1, "-Xptxas=-v")
-        procs.append(subprocess.Popen(cmd))
-    if any(p.wait() != 0 for p in procs):
+        procs.append((subprocess.Popen(cmd), o))
+    if any(p.wait() != 0 for p, _ in procs):
         raise RuntimeError("nvcc failed")
+    for _, o in procs:
+        os.utime(o, (started, started))
     subprocess.run([NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB + ".tmp", *objs],
                    check=True)
+    os.utime(LIB + ".tmp", (started, started))
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

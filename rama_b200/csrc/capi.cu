@@ -25,10 +25,15 @@ using namespace rama;
 
 namespace {
 
-constexpr int CLUSTER_CTAS = 8;               // CTAs of a cluster team (the portable maximum)
-constexpr int64_t CLUSTER_MIN_EDGES = 20000;   // smaller batch instances always run on one CTA
-constexpr int64_t SINGLE_CLUSTER_MIN = 4000;   // a single solve from this size on runs on a cluster
-constexpr int64_t GRID_MIN_EDGES = 100000;     // ... and from this size on on the whole GPU
+// Launch parameters a handle starts with (rama_tuning; the autotuner of
+// rama_b200/autotune.py replaces them with measured choices).  None of them
+// changes a result: every team computes the same solve.
+constexpr int DEFAULT_CLUSTER_CTAS = 8;            // CTAs of a cluster team (the portable maximum)
+constexpr int64_t DEFAULT_SINGLE_CLUSTER_MIN = 4000;  // a single solve from this size on runs on a cluster
+constexpr int64_t DEFAULT_SINGLE_GRID_MIN = 100000;   // ... and from this size on on the whole GPU
+constexpr int64_t DEFAULT_BATCH_CLUSTER_MIN = 20000;  // smaller batch instances always run on one CTA
+constexpr float DEFAULT_BATCH_CLUSTER_SHARE = 1.5f;   // ... larger ones on a cluster above this many
+                                                      // times the batch's edges per CTA
 
 thread_local std::string g_err;
 
@@ -86,7 +91,9 @@ struct rama_context {
     int step_ctas = 0;  // ... of k_step_grid
     int obj_ctas = 0;   // ... of k_objective
     int cta_per_sm = 0;
-    int cluster_max = 0;  // co-resident clusters of k_solve_mixed
+    int grid_per_sm_max = 0;  // occupancy maximum of k_solve_grid per SM
+    int cluster_cap[17] = {};  // co-resident clusters of k_solve_mixed by cluster size (0: not known yet)
+    rama_tuning tune{};
     int parse_ctas = 0;   // co-resident CTAs of k_parse_grid
     char *p_text = nullptr;  // device copy of text for rama_parse_multicut_host
     int64_t p_cap = 0;
@@ -162,13 +169,62 @@ int ensure_inst(rama_context *h, int32_t count)
     return RAMA_OK;
 }
 
-uint64_t ws_estimate(int64_t n_edges) { return (uint64_t)n_edges * 1024ull + (64ull << 20); }
+// Workspace bytes per edge: about 1 KiB covers a solve whose triangle budget
+// is at most twice the repulsive edges; each further unit of the budget
+// factor adds triangles at roughly 256 bytes each (sorts, message-passing
+// state).  A solve that still runs short reports the size it needed and is
+// run again with it.
+uint64_t ws_per_edge(float tri_factor)
+{
+    const double extra = tri_factor > 2.0f ? 256.0 * ((double)tri_factor - 2.0) : 0.0;
+    return 1024ull + (uint64_t)extra;
+}
+uint64_t ws_estimate(int64_t n_edges, float tri_factor = 2.0f)
+{
+    return (uint64_t)n_edges * ws_per_edge(tri_factor) + (64ull << 20);
+}
+uint64_t align4k(uint64_t b) { return (b + 4095) & ~uint64_t(4095); }
 // workspace slice of one instance of a batch
-uint64_t ws_slice(int64_t n_edges) { return ((uint64_t)n_edges * 1024ull + (1ull << 20) + 4095) & ~uint64_t(4095); }
+uint64_t ws_slice(int64_t n_edges, float tri_factor = 2.0f)
+{
+    return align4k((uint64_t)n_edges * ws_per_edge(tri_factor) + (1ull << 20));
+}
 
 // Launches the solve of the instances already in h->d_inst (queue order in
 // h->d_order).  team 2: one instance on the cooperative grid; otherwise the
 // first `ncluster` queue entries go to cluster teams and the rest to CTAs.
+// co-resident clusters of k_solve_mixed for a cluster size (0 if none fits)
+int cluster_capacity(rama_context *h, int size)
+{
+    if (size < 1 || size > 16) return 0;
+    if (!h->cluster_cap[size]) {
+        if (size > 8 && cudaFuncSetAttribute((const void *)k_solve_mixed,
+                                             cudaFuncAttributeNonPortableClusterSizeAllowed, 1) != cudaSuccess) {
+            cudaGetLastError();
+            h->cluster_cap[size] = -1;
+            return 0;
+        }
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(size);
+        cfg.blockDim = dim3(THREADS);
+        cfg.dynamicSmemBytes = SMEM;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = size;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int ncl = 0;
+        if (cudaOccupancyMaxActiveClusters(&ncl, (void *)k_solve_mixed, &cfg) != cudaSuccess) {
+            cudaGetLastError();
+            ncl = 0;
+        }
+        h->cluster_cap[size] = ncl > 0 ? ncl : -1;
+    }
+    return h->cluster_cap[size] > 0 ? h->cluster_cap[size] : 0;
+}
+
 int launch_solve(rama_context *h, int32_t count, int team, cudaStream_t st, int32_t ncluster = 0)
 {
     if (team == 2) {
@@ -176,9 +232,10 @@ int launch_solve(rama_context *h, int32_t count, int team, cudaStream_t st, int3
         void *args[] = {&L};
         CU(cudaLaunchCooperativeKernel((void *)k_solve_grid, dim3(h->grid_ctas), dim3(THREADS), args, SMEM, st));
     } else if (ncluster > 0) {
-        const int64_t want = (int64_t)ncluster * CLUSTER_CTAS + (count - ncluster);
-        const int64_t cap = (int64_t)std::max(1, h->cluster_max) * CLUSTER_CTAS;
-        const int64_t ctas = (std::min(want, cap) + CLUSTER_CTAS - 1) / CLUSTER_CTAS * CLUSTER_CTAS;
+        const int csz = h->tune.cluster_ctas;
+        const int64_t want = (int64_t)ncluster * csz + (count - ncluster);
+        const int64_t cap = (int64_t)std::max(1, cluster_capacity(h, csz)) * csz;
+        const int64_t ctas = (std::min(want, cap) + csz - 1) / csz * csz;
         CU(cudaMemsetAsync(h->d_queue, 0, sizeof(int32_t), st));
         MixedLaunch L{h->d_inst, h->d_order, count, ncluster, h->d_queue};
         cudaLaunchConfig_t cfg = {};
@@ -188,7 +245,7 @@ int launch_solve(rama_context *h, int32_t count, int team, cudaStream_t st, int3
         cfg.stream = st;
         cudaLaunchAttribute attr[1];
         attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = CLUSTER_CTAS;
+        attr[0].val.clusterDim.x = csz;
         attr[0].val.clusterDim.y = 1;
         attr[0].val.clusterDim.z = 1;
         cfg.attrs = attr;
@@ -212,7 +269,8 @@ int solve_one(rama_context *h, const int32_t *d_i, const int32_t *d_j, const flo
     if (h->b_active) return fail(RAMA_ERR_INVALID_ARG, "a batch is in flight on this handle (call rama_batch_wait)");
     Options o = to_opts(opts);
     int team = opts->team;
-    if (team < 1 || team > 3) team = n < SINGLE_CLUSTER_MIN ? 1 : (n < GRID_MIN_EDGES ? 3 : 2);
+    if (team < 1 || team > 3)
+        team = n < h->tune.single_cluster_min ? 1 : (n < h->tune.single_grid_min ? 3 : 2);
     int rc = ensure_inst(h, 1);
     if (rc) return rc;
     // timeline buffer
@@ -227,8 +285,8 @@ int solve_one(rama_context *h, const int32_t *d_i, const int32_t *d_j, const flo
         }
         tl = h->d_timeline;
     }
-    uint64_t need = h->ws_fixed ? h->ws_fixed : ws_estimate(n);
-    for (int attempt = 0; attempt < 4; ++attempt) {
+    uint64_t need = h->ws_fixed ? h->ws_fixed : ws_estimate(n, opts->tri_memory_factor);
+    for (int attempt = 0; attempt < 8; ++attempt) {
         rc = ensure_ws(h, need);
         if (rc) return rc;
         Instance hi{};
@@ -257,13 +315,24 @@ int solve_one(rama_context *h, const int32_t *d_i, const int32_t *d_j, const flo
         CU(cudaStreamSynchronize(st));
         float ms = 0;
         cudaEventElapsedTime(&ms, h->ev0, h->ev1);
-        if ((ho.status & ERR_ARENA) && !h->ws_fixed) {
+        // A solve that ran out of workspace runs again with more.  That
+        // includes a dual that fell back to the trivial bound when a larger
+        // workspace would have held its triangles: the reference allocates
+        // device memory as it goes and falls back only when the device has
+        // none left (src/dual_solver.cu:58-61), and so does this loop.
+        const bool short_ws =
+            (ho.status & ERR_ARENA) || (ho.dual_oom && (uint64_t)ho.arena_want > h->ws_bytes);
+        if (short_ws && !h->ws_fixed) {
             size_t fr = 0, tot = 0;
             cudaMemGetInfo(&fr, &tot);
-            uint64_t grow = std::max<uint64_t>(need * 2, h->ws_bytes * 2);
-            if (h->ws_bytes >= (uint64_t)((double)(fr + h->ws_bytes) * 0.9)) break;
-            need = grow;
-            continue;
+            const uint64_t avail = (uint64_t)((double)(fr + h->ws_bytes) * 0.9);
+            if (h->ws_bytes < avail) {
+                const uint64_t want = (uint64_t)((double)ho.arena_want * 1.25);
+                need = std::min<uint64_t>(avail, std::max<uint64_t>(h->ws_bytes * 2, want));
+                continue;
+            }
+            if (ho.status & ERR_ARENA) break;
+            // the device is full: keep the trivial bound, as the reference does
         }
         h->stats.rounds = ho.rounds;
         h->stats.matching_rounds = ho.matching_rounds;
@@ -279,7 +348,7 @@ int solve_one(rama_context *h, const int32_t *d_i, const int32_t *d_j, const flo
         {
             int64_t pr[2 * PH_COUNT];
             CU(cudaMemcpy(pr, h->d_prof, sizeof(pr), cudaMemcpyDeviceToHost));
-            for (int k = 0; k < PH_COUNT && k < 10; ++k) {
+            for (int k = 0; k < PH_COUNT && k < 16; ++k) {
                 h->stats.phase_ms[k] = 1e-6 * (double)pr[k];
                 h->stats.phase_bytes[k] = (double)pr[PH_COUNT + k];
             }
@@ -374,7 +443,14 @@ int rama_create(int device, uint64_t workspace_bytes, rama_handle *out)
         delete h;
         return fail(RAMA_ERR_CUDA, "solver kernel does not fit on an SM");
     }
+    h->grid_per_sm_max = per_sm;
     h->grid_ctas = per_sm * h->sms;
+    h->tune.grid_ctas_per_sm = per_sm;
+    h->tune.cluster_ctas = DEFAULT_CLUSTER_CTAS;
+    h->tune.single_cluster_min = DEFAULT_SINGLE_CLUSTER_MIN;
+    h->tune.single_grid_min = DEFAULT_SINGLE_GRID_MIN;
+    h->tune.batch_cluster_min = DEFAULT_BATCH_CLUSTER_MIN;
+    h->tune.batch_cluster_share = DEFAULT_BATCH_CLUSTER_SHARE;
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_grid, THREADS, SMEM));
     h->step_ctas = std::max(1, per_sm) * h->sms;
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_objective, THREADS, SMEM));
@@ -384,21 +460,9 @@ int rama_create(int device, uint64_t workspace_bytes, rama_handle *out)
     int per_sm_cta = 0;
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_cta, k_solve_cta, THREADS, SMEM));
     h->cta_per_sm = std::max(1, per_sm_cta);
-    {
-        cudaLaunchConfig_t cfg = {};
-        cfg.gridDim = dim3(CLUSTER_CTAS);
-        cfg.blockDim = dim3(THREADS);
-        cfg.dynamicSmemBytes = SMEM;
-        cudaLaunchAttribute attr[1];
-        attr[0].id = cudaLaunchAttributeClusterDimension;
-        attr[0].val.clusterDim.x = CLUSTER_CTAS;
-        attr[0].val.clusterDim.y = 1;
-        attr[0].val.clusterDim.z = 1;
-        cfg.attrs = attr;
-        cfg.numAttrs = 1;
-        int ncl = 0;
-        CU(cudaOccupancyMaxActiveClusters(&ncl, (void *)k_solve_mixed, &cfg));
-        h->cluster_max = std::max(1, ncl);
+    if (cluster_capacity(h, DEFAULT_CLUSTER_CTAS) < 1) {
+        delete h;
+        return fail(RAMA_ERR_CUDA, "no cluster of the solver kernel fits on the device");
     }
     CU(cudaMalloc(&h->d_queue, sizeof(int32_t) * 4));
     CU(cudaMalloc(&h->d_step, sizeof(rama_step_args)));
@@ -572,7 +636,8 @@ int rama_batch_launch(rama_handle h, const int32_t *d_i, const int32_t *d_j, con
         int64_t total_edges = 0;
         for (int32_t k = 0; k < count; ++k) total_edges += h->b_in[k].n;
         const int64_t per_cta = total_edges / std::max(1, h->sms * h->cta_per_sm);
-        const int64_t auto_min = std::max<int64_t>(CLUSTER_MIN_EDGES, per_cta + per_cta / 2);
+        const int64_t auto_min = std::max<int64_t>(h->tune.batch_cluster_min,
+                                                   (int64_t)((double)per_cta * h->tune.batch_cluster_share));
         for (int32_t k = 0; k < count; ++k) {
             const int tm = opts[opts_count == 1 ? 0 : k].team;
             h->b_cluster[k] = (tm == 2 || tm == 3 || ((tm < 1 || tm > 3) && h->b_in[k].n >= auto_min)) ? 1 : 0;
@@ -588,7 +653,7 @@ int rama_batch_launch(rama_handle h, const int32_t *d_i, const int32_t *d_j, con
     // every instance owns a workspace slice sized from its edge count; their
     // sum is the batch's device footprint
     uint64_t total = 0;
-    for (int32_t k = 0; k < count; ++k) total += ws_slice(h->b_in[k].n);
+    for (int32_t k = 0; k < count; ++k) total += ws_slice(h->b_in[k].n, h->b_in[k].opts.tri_memory_factor);
     // a handle with a fixed workspace allocates all of it once and admits
     // batches up to that size
     if (h->ws_fixed && total > h->ws_fixed) return fail(RAMA_ERR_OOM, "batch exceeds the handle's fixed workspace");
@@ -599,7 +664,7 @@ int rama_batch_launch(rama_handle h, const int32_t *d_i, const int32_t *d_j, con
         uint64_t off = 0;
         for (int32_t k = 0; k < count; ++k) {
             h->b_in[k].ws = h->ws + off;
-            h->b_in[k].ws_bytes = ws_slice(h->b_in[k].n);
+            h->b_in[k].ws_bytes = ws_slice(h->b_in[k].n, h->b_in[k].opts.tri_memory_factor);
             off += h->b_in[k].ws_bytes;
         }
     }
@@ -637,14 +702,20 @@ int rama_batch_wait(rama_handle h, int64_t *num_labels, double *lbs, int32_t *st
     float ms = 0;
     cudaEventElapsedTime(&ms, h->ev0, h->ev1);
     std::vector<Instance> out(h->b_host, h->b_host + count);
-    // instances that ran out of workspace are solved again with twice the slice
-    for (int attempt = 0; attempt < 3; ++attempt) {
+    // instances that ran out of workspace (a dual fallback included, when a
+    // larger slice would have held it) are solved again with a larger slice:
+    // twice the old one, or what the refused allocation needed
+    auto bigger = [&](int32_t k) {
+        return align4k(std::max<uint64_t>(h->b_in[k].ws_bytes * 2, (uint64_t)((double)out[k].arena_want * 1.25)));
+    };
+    for (int attempt = 0; attempt < 4; ++attempt) {
         std::vector<int32_t> redo;
         for (int32_t k = 0; k < count; ++k)
-            if (out[k].status & ERR_ARENA) redo.push_back(k);
+            if ((out[k].status & ERR_ARENA) || (out[k].dual_oom && (uint64_t)out[k].arena_want > h->b_in[k].ws_bytes))
+                redo.push_back(k);
         if (redo.empty()) break;
         uint64_t total = 0;
-        for (int32_t k : redo) total += h->b_in[k].ws_bytes * 2;
+        for (int32_t k : redo) total += bigger(k);
         if (h->ws_fixed && total > h->ws_fixed) break;  // they stay out of workspace
         int rc = ensure_ws(h, total);
         if (rc) return rc;
@@ -658,7 +729,7 @@ int rama_batch_wait(rama_handle h, int64_t *num_labels, double *lbs, int32_t *st
         uint64_t off = 0;
         for (size_t q = 0; q < redo.size(); ++q) {
             Instance &x = h->b_in[redo[q]];
-            x.ws_bytes *= 2;
+            x.ws_bytes = bigger(redo[q]);
             x.ws = h->ws + off;
             off += x.ws_bytes;
             if (off > h->ws_bytes) return fail(RAMA_ERR_OOM, "workspace exhausted");
@@ -700,6 +771,32 @@ int rama_solve_batch(rama_handle h, const int32_t *d_i, const int32_t *d_j, cons
     int rc = rama_batch_launch(h, d_i, d_j, d_costs, edge_offsets, count, opts, 1, d_labels, label_offsets, stream);
     if (rc) return rc;
     return rama_batch_wait(h, num_labels, lbs, status);
+}
+
+int rama_get_tuning(rama_handle h, rama_tuning *out)
+{
+    if (!h || !out) return fail(RAMA_ERR_INVALID_ARG, "bad arguments");
+    *out = h->tune;
+    return RAMA_OK;
+}
+
+int rama_set_tuning(rama_handle h, const rama_tuning *t)
+{
+    if (!h || !t) return fail(RAMA_ERR_INVALID_ARG, "bad arguments");
+    CU(cudaSetDevice(h->device));
+    if (t->grid_ctas_per_sm < 1 || t->grid_ctas_per_sm > h->grid_per_sm_max)
+        return fail(RAMA_ERR_INVALID_ARG,
+                    "grid_ctas_per_sm must lie in [1, " + std::to_string(h->grid_per_sm_max) + "]");
+    const int c = t->cluster_ctas;
+    if (!(c == 2 || c == 4 || c == 8 || c == 16)) return fail(RAMA_ERR_INVALID_ARG, "cluster_ctas must be 2, 4, 8 or 16");
+    if (cluster_capacity(h, c) < 1)
+        return fail(RAMA_ERR_INVALID_ARG, "no cluster of " + std::to_string(c) + " CTAs fits on this device");
+    if (t->single_cluster_min < 0 || t->single_grid_min < 0 || t->batch_cluster_min < 0 ||
+        !(t->batch_cluster_share > 0.0f))
+        return fail(RAMA_ERR_INVALID_ARG, "thresholds must be non-negative and the share positive");
+    h->tune = *t;
+    h->grid_ctas = t->grid_ctas_per_sm * h->sms;
+    return RAMA_OK;
 }
 
 int rama_get_stats(rama_handle h, rama_stats *out)
@@ -796,7 +893,8 @@ int rama_step(rama_handle h, rama_step_args *a, void *stream)
     CU(cudaSetDevice(h->device));
     cudaStream_t st = (cudaStream_t)stream;
     int64_t scale = std::max<int64_t>({a->n, a->m, a->T * 3, a->adj_len, (int64_t)a->num_nodes, a->map_size});
-    int rc = ensure_ws(h, h->ws_fixed ? h->ws_fixed : ws_estimate(scale) + (uint64_t)a->num_nodes * 64);
+    int rc = ensure_ws(h, h->ws_fixed ? h->ws_fixed
+                                      : ws_estimate(scale, a->tri_memory_factor) + (uint64_t)a->num_nodes * 64);
     if (rc) return rc;
     a->status = 0;
     CU(cudaMemcpyAsync(h->d_step, a, sizeof(rama_step_args), cudaMemcpyHostToDevice, st));

@@ -291,7 +291,9 @@ __device__ void conflicted_cycles(const Team &t, Scratch &sc, char *sm, const Gr
         [&](int64_t e, int64_t pre, int64_t v) {
             if (v) ridx[pre] = e;
         });
+    prof_mark(t, sc, PH_CYCLES);
     Csr C = build_symmetric_csr(t, sc, sm, A, N, [&](int64_t e) { return A.cost[e] > pos_tol; }, false);
+    prof_mark(t, sc, PH_CSR);
     const int64_t budget = (int64_t)(int32_t)(tri_factor * (float)Rall);  // (:247)
     tb.budget = budget < 0 ? 0 : budget;
     tb.t1 = sc.arena.take<int32_t>(tb.budget + 1);

@@ -339,6 +339,7 @@ __device__ Graph graph_contract(const Team &t, Scratch &sc, char *sm, const Grap
         sc.arena.release(m);
         return graph_contract_sorted(t, sc, sm, A, map, map_max, bad);
     }
+    prof_mark(t, sc, PH_CONTRACT_SORT);
     // 3. runs of every bucket
     int32_t mxhi = -1, lastb = -1;
     for (int64_t b = t.rank(); b < nbk; b += t.size()) {

@@ -74,6 +74,7 @@ __device__ int32_t matching_contraction_map(const Team &t, Scratch &sc, char *sm
             sc.arena.release(mark);
             return 0;
         }
+        prof_mark(t, sc, PH_MATCHING);
         int64_t ncand = 0;      // entries of the list read by this iteration
         int32_t ntouch_prev = 0;  // vertices touched by the previous iteration
         for (int it = 0; it < 10; ++it) {
@@ -82,54 +83,104 @@ __device__ int32_t matching_contraction_map(const Team &t, Scratch &sc, char *sm
             int32_t *cnt_next = flags + 16 + 2 * (it & 7);  // [0]: next list, [1]: touched
             int32_t *cnt_clear = flags + 16 + 2 * ((it + 1) & 7);
             // pick_best_neighbour: every live candidate offers itself to both
-            // ends; it stays a candidate for the next iteration
-            auto offer_edge = [&](int32_t u, int32_t v, uint32_t hb, bool live) {
-                unsigned long long ou = 0, ov = 0;
-                if (live) {
-                    const unsigned long long hi = (unsigned long long)hb << 32;
-                    ou = atomicMax(&cur_offer[u], hi | (unsigned long long)(~(uint32_t)v));
-                    ov = atomicMax(&cur_offer[v], hi | (unsigned long long)(~(uint32_t)u));
+            // ends and stays a candidate for the next iteration.  A lane takes
+            // MI edges at once (independent loads, gathers and atomics in
+            // flight together); a warp reserves list space once per 32 * MI.
+            constexpr int MI = 4;
+            auto offer_batch = [&](const int32_t (&u)[MI], const int32_t (&v)[MI], const uint32_t (&hb)[MI],
+                                   const bool (&live)[MI]) {
+                bool fu[MI], fv[MI];
+#pragma unroll
+                for (int k = 0; k < MI; ++k) {
+                    fu[k] = fv[k] = false;
+                    if (live[k]) {
+                        const unsigned long long hi = (unsigned long long)hb[k] << 32;
+                        fu[k] = atomicMax(&cur_offer[u[k]], hi | (unsigned long long)(~(uint32_t)v[k])) == 0ull;
+                        fv[k] = atomicMax(&cur_offer[v[k]], hi | (unsigned long long)(~(uint32_t)u[k])) == 0ull;
+                    }
                 }
-                // append the edge to the next list and first-touched vertices
-                // to the touched list (one atomic per warp for each)
-                const unsigned bl = __ballot_sync(FULL, live);
-                int32_t base = 0;
-                if (lane_id() == 0 && bl) base = atomicAdd(&cnt_next[0], __popc(bl));
-                base = __shfl_sync(FULL, base, 0);
-                if (live) {
-                    const int32_t p = base + __popc(bl & lanemask_lt());
-                    cand[nxt][p] = make_int2(u, v);
-                    cbits[nxt][p] = hb;
+                int nl = 0, nt = 0;
+#pragma unroll
+                for (int k = 0; k < MI; ++k) {
+                    nl += live[k];
+                    nt += fu[k] + fv[k];
                 }
-                const bool fu = live && ou == 0ull, fv = live && ov == 0ull;
-                const unsigned bu = __ballot_sync(FULL, fu), bv = __ballot_sync(FULL, fv);
-                int32_t tb = 0;
-                if (lane_id() == 0 && (bu | bv)) tb = atomicAdd(&cnt_next[1], __popc(bu) + __popc(bv));
-                tb = __shfl_sync(FULL, tb, 0);
-                if (fu) touched[cur][tb + __popc(bu & lanemask_lt())] = u;
-                if (fv) touched[cur][tb + __popc(bu) + __popc(bv & lanemask_lt())] = v;
+                // one reservation per warp for both lists: lane prefixes by
+                // a warp scan of (touched << 16 | list) counts
+                const int packed = (nt << 16) | nl;
+                const int incl = warp_incl_scan(packed);
+                const int tot = __shfl_sync(FULL, incl, 31);
+                int lbase = 0, tbase = 0;
+                if (lane_id() == 0) {
+                    if (tot & 0xffff) lbase = atomicAdd(&cnt_next[0], tot & 0xffff);
+                    if (tot >> 16) tbase = atomicAdd(&cnt_next[1], tot >> 16);
+                }
+                lbase = __shfl_sync(FULL, lbase, 0) + ((incl - packed) & 0xffff);
+                tbase = __shfl_sync(FULL, tbase, 0) + ((incl - packed) >> 16);
+#pragma unroll
+                for (int k = 0; k < MI; ++k) {
+                    if (live[k]) {
+                        cand[nxt][lbase] = make_int2(u[k], v[k]);
+                        cbits[nxt][lbase] = hb[k];
+                        ++lbase;
+                    }
+                    if (fu[k]) touched[cur][tbase++] = u[k];
+                    if (fv[k]) touched[cur][tbase++] = v[k];
+                }
             };
+            const int64_t stride = (int64_t)team_nwarps(t) * 32 * MI;
             if (it == 0) {
-                for (int64_t base = (int64_t)t.rank() - lane_id(); base < A.n; base += t.size()) {
-                    const int64_t e = base + lane_id();
-                    const float c = e < A.n ? A.cost[e] : 0.0f;
-                    const bool live = e < A.n && c > thresh && A.row[e] != A.col[e];
-                    offer_edge(live ? A.row[e] : 0, live ? A.col[e] : 0, float_ordered(c), live);
+                for (int64_t base = (int64_t)team_warp(t) * 32 * MI; base < A.n; base += stride) {
+                    int32_t u[MI], v[MI];
+                    uint32_t hb[MI];
+                    bool live[MI];
+                    float c[MI];
+#pragma unroll
+                    for (int k = 0; k < MI; ++k) {
+                        const int64_t e = base + k * 32 + lane_id();
+                        c[k] = e < A.n ? A.cost[e] : 0.0f;
+                    }
+#pragma unroll
+                    for (int k = 0; k < MI; ++k) {
+                        const int64_t e = base + k * 32 + lane_id();
+                        live[k] = e < A.n && c[k] > thresh;
+                        u[k] = live[k] ? A.row[e] : 0;
+                        v[k] = live[k] ? A.col[e] : 0;
+                        hb[k] = float_ordered(c[k]);
+                    }
+#pragma unroll
+                    for (int k = 0; k < MI; ++k) live[k] = live[k] && u[k] != v[k];
+                    offer_batch(u, v, hb, live);
                 }
             } else {
                 const int2 *L = cand[cur];
                 const uint32_t *LB = cbits[cur];
-                for (int64_t base = (int64_t)t.rank() - lane_id(); base < ncand; base += t.size()) {
-                    const int64_t q = base + lane_id();
-                    int2 uv = make_int2(0, 0);
-                    uint32_t hb = 0;
-                    bool live = false;
-                    if (q < ncand) {
-                        uv = L[q];
-                        hb = LB[q];
-                        live = !matched[uv.x] && !matched[uv.y];
+                for (int64_t base = (int64_t)team_warp(t) * 32 * MI; base < ncand; base += stride) {
+                    int32_t u[MI], v[MI];
+                    uint32_t hb[MI];
+                    bool live[MI];
+#pragma unroll
+                    for (int k = 0; k < MI; ++k) {
+                        const int64_t q = base + k * 32 + lane_id();
+                        int2 uv = make_int2(0, 0);
+                        hb[k] = 0;
+                        if (q < ncand) {
+                            uv = L[q];
+                            hb[k] = LB[q];
+                        }
+                        u[k] = uv.x;
+                        v[k] = uv.y;
+                        live[k] = q < ncand;
                     }
-                    offer_edge(uv.x, uv.y, hb, live);
+                    int32_t mu[MI], mv[MI];
+#pragma unroll
+                    for (int k = 0; k < MI; ++k) {
+                        mu[k] = live[k] ? matched[u[k]] : 1;
+                        mv[k] = live[k] ? matched[v[k]] : 1;
+                    }
+#pragma unroll
+                    for (int k = 0; k < MI; ++k) live[k] = live[k] && !mu[k] && !mv[k];
+                    offer_batch(u, v, hb, live);
                 }
             }
             if (t.rank() < 2) cnt_clear[t.rank()] = 0;  // counters of the iteration after next
@@ -172,6 +223,7 @@ __device__ int32_t matching_contraction_map(const Team &t, Scratch &sc, char *sm
             // the next offer pass reads `matched` after this sync
         }
         sc.arena.release(lm);
+        prof_mark(t, sc, PH_MATCH_ITER);
     }
     compress_labels(t, sc, sm, nm, M, M - 1, map_out);
     sc.arena.release(mark);

@@ -58,6 +58,7 @@ __device__ __forceinline__ Scratch scratch_over(char *base, uint64_t bytes)
     sc.arena.lo = 2 * SCRATCH_PART_BYTES + 256;
     sc.arena.top = sc.arena.cap;
     sc.arena.peak = sc.arena.lo;
+    sc.arena.want = 0;
     sc.arena.failed = 0;
     return sc;
 }
@@ -76,7 +77,10 @@ enum Phase : int {
     PH_WOC = 6,
     PH_CONTRACT = 7,
     PH_OTHER = 8,
-    PH_COUNT = 10
+    PH_MATCH_ITER = 9,    // the offer / match iterations of a matching round
+    PH_CONTRACT_SORT = 10,  // the bucket sort of a contraction
+    PH_CSR = 11,          // symmetric CSR builds (cycle search, forest)
+    PH_COUNT = 16
 };
 
 __device__ __forceinline__ uint64_t prof_now()

@@ -49,6 +49,7 @@ struct Instance {
     int32_t dual_oom;
     int64_t triangles_initial;
     int64_t arena_peak;
+    int64_t arena_want;      // workspace bytes a refused allocation needed (0: none refused)
     int64_t edges_after_dual;
     double alg_bytes;
 };
@@ -211,6 +212,7 @@ __device__ void solve_instance(const Team &t, char *sm, Scratch sc, Instance *io
         io->dual_oom = oom;
         io->triangles_initial = ntri;
         io->arena_peak = (int64_t)sc.arena.peak;
+        io->arena_want = (int64_t)sc.arena.want;
         io->edges_after_dual = eafter;
         io->alg_bytes = sc.alg_bytes;
     }

@@ -90,6 +90,7 @@ struct Arena {
     uint64_t top;  // first byte of the graph slot
     uint64_t cap;  // usable bytes (a guard area of 256 B follows)
     uint64_t peak;
+    uint64_t want;  // workspace bytes the largest refused allocation needed (0: none refused)
     int failed;
 
     __device__ __forceinline__ bool ok() const { return !failed; }
@@ -99,6 +100,9 @@ struct Arena {
         uint64_t a = (lo + 255) & ~uint64_t(255);
         uint64_t e = a + n * sizeof(T);
         if (failed || e > top) {
+            // the temporaries up to e, the graph slot above them and the guard
+            const uint64_t need = e + (cap - top) + 512;
+            if (!failed && need > want) want = need;
             failed = 1;
             return reinterpret_cast<T *>(base + cap);  // guard area
         }
