@@ -205,7 +205,9 @@ int rama_parse_multicut_host(rama_handle h, const char *text, int64_t len, int32
  * rama_b200/autotune.py measures better ones per device and sets them.  No
  * counterpart in the reference (its launches have fixed shapes). */
 typedef struct {
-    int32_t grid_ctas_per_sm;    /* CTAs per SM of the whole-GPU solve (1 .. the occupancy maximum) */
+    int32_t grid_ctas_per_sm;    /* CTAs per SM of the whole-GPU solve (1 .. the occupancy maximum) ... */
+    int32_t grid_small_ctas_per_sm; /* ... and of one of fewer than grid_small_max edges */
+    int64_t grid_small_max;
     int32_t cluster_ctas;        /* CTAs of a cluster team: 2, 4, 8 or 16 */
     int64_t single_cluster_min;  /* a single solve of at least this many edges runs on a cluster ... */
     int64_t single_grid_min;     /* ... and from this many on on the whole GPU (else on one CTA) */

@@ -63,6 +63,8 @@ class RamaStats(C.Structure):
 class RamaTuning(C.Structure):
     _fields_ = [
         ("grid_ctas_per_sm", C.c_int32),
+        ("grid_small_ctas_per_sm", C.c_int32),
+        ("grid_small_max", C.c_int64),
         ("cluster_ctas", C.c_int32),
         ("single_cluster_min", C.c_int64),
         ("single_grid_min", C.c_int64),

@@ -7,9 +7,10 @@ thread-block cluster of 2 to 16 CTAs, or the whole GPU -- so the choice of
 team and of its size only decides how fast a solve runs.  The handle's
 built-in choices are guesses; this module measures them on the device:
 
-* grid_ctas_per_sm: CTAs per SM of the whole-GPU solve (fewer CTAs take
-  cheaper grid barriers, more CTAs hide more memory latency), timed on a
-  large 3-D grid;
+* grid_ctas_per_sm, grid_small_ctas_per_sm, grid_small_max: CTAs per SM of
+  the whole-GPU solve, for large graphs and for graphs below a size (fewer
+  CTAs take cheaper grid barriers, more CTAs hide more memory latency), timed
+  on 3-D grids of growing size;
 * cluster_ctas: the cluster size, timed on mid-size Delaunay graphs;
 * single_cluster_min / single_grid_min: where a single solve moves from one
   CTA to a cluster and from a cluster to the whole GPU -- each team is timed
@@ -40,8 +41,8 @@ import numpy as np
 from . import _lib
 from . import instances as I
 
-KNOBS = ("grid_ctas_per_sm", "cluster_ctas", "single_cluster_min", "single_grid_min", "batch_cluster_min",
-         "batch_cluster_share")
+KNOBS = ("grid_ctas_per_sm", "grid_small_ctas_per_sm", "grid_small_max", "cluster_ctas", "single_cluster_min",
+         "single_grid_min", "batch_cluster_min", "batch_cluster_share")
 
 
 def cache_path() -> str:
@@ -185,15 +186,24 @@ def tune(device: int = 0, budget_s: float = 60.0, quick: bool = False) -> dict:
     tables: dict = {}
     chosen = dict(base)
 
-    # whole-GPU solves: CTAs per SM on a large 3-D grid
-    big = I.grid3d_longrange(96, 96, 48, seed=7) if not quick else I.grid3d_longrange(48, 48, 24, seed=7)
+    # whole-GPU solves: CTAs per SM, on 3-D grids of growing size (fewer
+    # CTAs take cheaper grid barriers, which pays on smaller graphs; more
+    # CTAs keep more memory traffic in flight, which pays on larger ones)
+    dims = [(48, 48, 24), (96, 96, 48), (160, 160, 64)] if not quick else [(32, 32, 16), (64, 64, 32)]
     opts = list(range(1, int(base["grid_ctas_per_sm"]) + 1))
-    tg = {}
-    for g in opts:
-        tr.set(grid_ctas_per_sm=g)
-        tg[g] = tr.solve("grid", big, "PD", team=2)
-    chosen["grid_ctas_per_sm"] = pick_fastest(tg)
-    tables["grid_ctas_per_sm"] = tg
+    gsizes, gt = [], {g: [] for g in opts}
+    for k, (nx, ny, nz) in enumerate(dims):
+        inst = I.grid3d_longrange(nx, ny, nz, seed=7)
+        gsizes.append(len(inst[2]))
+        for g in opts:
+            tr.set(grid_ctas_per_sm=g, grid_small_ctas_per_sm=g, grid_small_max=0)
+            gt[g].append(tr.solve("grid%d" % k, inst, "PD", team=2))
+    large = pick_fastest({g: gt[g][-1] for g in opts})
+    small = pick_fastest({g: gt[g][0] for g in opts})
+    chosen["grid_ctas_per_sm"] = large
+    chosen["grid_small_ctas_per_sm"] = small
+    chosen["grid_small_max"] = 0 if small == large else crossover(gsizes, gt[small], gt[large], 0)
+    tables["grid"] = {"edges": gsizes, **{"ctas_per_sm_%d_ms" % g: gt[g] for g in opts}}
     tr.set(**chosen)
 
     # cluster size on mid-size graphs

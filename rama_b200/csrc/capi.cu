@@ -225,12 +225,15 @@ int cluster_capacity(rama_context *h, int size)
     return h->cluster_cap[size] > 0 ? h->cluster_cap[size] : 0;
 }
 
-int launch_solve(rama_context *h, int32_t count, int team, cudaStream_t st, int32_t ncluster = 0)
+int launch_solve(rama_context *h, int32_t count, int team, cudaStream_t st, int32_t ncluster = 0,
+                 int64_t grid_edges = 0)
 {
     if (team == 2) {
         GridLaunch L{h->d_inst, h->ws, h->ws_bytes};
         void *args[] = {&L};
-        CU(cudaLaunchCooperativeKernel((void *)k_solve_grid, dim3(h->grid_ctas), dim3(THREADS), args, SMEM, st));
+        const int per_sm = grid_edges < h->tune.grid_small_max ? h->tune.grid_small_ctas_per_sm
+                                                                : h->tune.grid_ctas_per_sm;
+        CU(cudaLaunchCooperativeKernel((void *)k_solve_grid, dim3(per_sm * h->sms), dim3(THREADS), args, SMEM, st));
     } else if (ncluster > 0) {
         const int csz = h->tune.cluster_ctas;
         const int64_t want = (int64_t)ncluster * csz + (count - ncluster);
@@ -307,7 +310,7 @@ int solve_one(rama_context *h, const int32_t *d_i, const int32_t *d_j, const flo
         CU(cudaMemcpyAsync(h->d_inst, &hi, sizeof(Instance), cudaMemcpyHostToDevice, st));
         CU(cudaMemcpyAsync(h->d_order, &zero, sizeof(int32_t), cudaMemcpyHostToDevice, st));
         CU(cudaEventRecord(h->ev0, st));
-        rc = launch_solve(h, 1, team, st, team == 3 ? 1 : 0);
+        rc = launch_solve(h, 1, team, st, team == 3 ? 1 : 0, n);
         if (rc) return rc;
         CU(cudaEventRecord(h->ev1, st));
         Instance ho{};
@@ -446,6 +449,8 @@ int rama_create(int device, uint64_t workspace_bytes, rama_handle *out)
     h->grid_per_sm_max = per_sm;
     h->grid_ctas = per_sm * h->sms;
     h->tune.grid_ctas_per_sm = per_sm;
+    h->tune.grid_small_ctas_per_sm = per_sm;
+    h->tune.grid_small_max = 0;
     h->tune.cluster_ctas = DEFAULT_CLUSTER_CTAS;
     h->tune.single_cluster_min = DEFAULT_SINGLE_CLUSTER_MIN;
     h->tune.single_grid_min = DEFAULT_SINGLE_GRID_MIN;
@@ -784,9 +789,10 @@ int rama_set_tuning(rama_handle h, const rama_tuning *t)
 {
     if (!h || !t) return fail(RAMA_ERR_INVALID_ARG, "bad arguments");
     CU(cudaSetDevice(h->device));
-    if (t->grid_ctas_per_sm < 1 || t->grid_ctas_per_sm > h->grid_per_sm_max)
+    if (t->grid_ctas_per_sm < 1 || t->grid_ctas_per_sm > h->grid_per_sm_max || t->grid_small_ctas_per_sm < 1 ||
+        t->grid_small_ctas_per_sm > h->grid_per_sm_max || t->grid_small_max < 0)
         return fail(RAMA_ERR_INVALID_ARG,
-                    "grid_ctas_per_sm must lie in [1, " + std::to_string(h->grid_per_sm_max) + "]");
+                    "grid CTAs per SM must lie in [1, " + std::to_string(h->grid_per_sm_max) + "]");
     const int c = t->cluster_ctas;
     if (!(c == 2 || c == 4 || c == 8 || c == 16)) return fail(RAMA_ERR_INVALID_ARG, "cluster_ctas must be 2, 4, 8 or 16");
     if (cluster_capacity(h, c) < 1)
@@ -795,7 +801,6 @@ int rama_set_tuning(rama_handle h, const rama_tuning *t)
         !(t->batch_cluster_share > 0.0f))
         return fail(RAMA_ERR_INVALID_ARG, "thresholds must be non-negative and the share positive");
     h->tune = *t;
-    h->grid_ctas = t->grid_ctas_per_sm * h->sms;
     return RAMA_OK;
 }
 
