@@ -281,18 +281,17 @@ __device__ Graph graph_contract_sorted(const Team &t, Scratch &sc, char *sm, con
 // remove_diagonal) by buckets of the new row:
 //   1. each edge's contracted endpoints (lo, hi) are computed once, with its
 //      slot in bucket lo;
-//   2. the bucket sort orders every bucket by (hi, edge index) and carries the
-//      edge's cost bits along (no gather afterwards);
-//   3. one thread per bucket walks its runs of equal hi: RSUM of a run's
-//      costs in edge order (runs of more than 32 by a warp afterwards), the
-//      diagonal run's sum checked for a bad contraction, the others written
-//      back into the bucket's own range; the largest hi and the last
-//      non-empty bucket give the dims (taken before the diagonal goes, as the
-//      reference does);
-//   4. a scan of the per-bucket counts places the rows, and the edges are
-//      written straight into the graph slot at the top of the arena (the old
-//      graph there is dead by then), with the smallest cost for the cycle
-//      search.
+//   2. the bucket sort orders every bucket by (hi, edge index), carrying the
+//      edge's cost bits and its bucket along (no gather afterwards);
+//   3. one scan over the sorted edges finds the heads of the runs of equal
+//      (lo, hi) and numbers the runs that are not self-loops; the head's
+//      thread sums its run (RSUM in edge order; runs of more than 32 by a
+//      warp afterwards) and writes the edge straight into the graph slot at
+//      the top of the arena (the old graph there is dead by then), or checks
+//      a self-loop's sum for a bad contraction;
+//   4. one pass over the new edges gives the largest column and the smallest
+//      cost; the rows are the last bucket + 1 (dims are taken before the
+//      diagonal goes, as the reference does).
 // A bucket of more than BUCKET_MAX edges sends the contraction to
 // graph_contract_sorted (one radix sort of the packed keys).  Both give the
 // same graph bit for bit.
@@ -302,27 +301,22 @@ __device__ Graph graph_contract(const Team &t, Scratch &sc, char *sm, const Grap
 {
     const int64_t n = A.n;
     Graph out = A;
-    if (n >= (int64_t(1) << 31)) return graph_contract_sorted(t, sc, sm, A, map, map_max, bad);
+    if (n == 0 || n >= (int64_t(1) << 31)) return graph_contract_sorted(t, sc, sm, A, map, map_max, bad);
     const int32_t nbk = map_max + 1;
     uint64_t m = sc.arena.mark();
     int2 *lohi = sc.arena.take<int2>(n + 1);
     uint64_t *sk = sc.arena.take<uint64_t>(n + 1);
     int32_t *sbits = sc.arena.take<int32_t>(n + 1);
+    int32_t *sbk = sc.arena.take<int32_t>(n + 1);
     int32_t *bst = sc.arena.take<int32_t>((int64_t)nbk + 2);
-    int32_t *cnt = sc.arena.take<int32_t>((int64_t)nbk + 2);
-    int32_t *opos = sc.arena.take<int32_t>((int64_t)nbk + 2);
-    int32_t *rcol = sc.arena.take<int32_t>(n + 1);
-    float *rcost = sc.arena.take<float>(n + 1);
     int4 *longq = sc.arena.take<int4>(n / 33 + 2);
-    // [0] bad, [1] long runs, [2] max hi, [3] last non-empty bucket, [4] smallest cost (ordered bits)
+    // [0] bad, [1] long runs, [2] largest self-loop column
     int32_t *fl = sc.arena.take<int32_t>(8);
     if (!sc.arena.ok()) return out;
     if (t.rank() == 0) {
         fl[0] = 0;
         fl[1] = 0;
         fl[2] = -1;
-        fl[3] = -1;
-        fl[4] = (int32_t)0xffffffffu;
     }
     const bool done = team_bucket_sort_ex(
         t, sc, sm, n, nbk,
@@ -334,52 +328,62 @@ __device__ Graph graph_contract(const Team &t, Scratch &sc, char *sm, const Grap
         },
         [&](int64_t e) { return lohi[e].x; },
         [&](int64_t e) -> uint64_t { return ((uint64_t)(uint32_t)lohi[e].y << 32) | (uint64_t)e; },
-        [&](int64_t e) { return __float_as_int(A.cost[e]); }, sk, sbits, bst);
+        [&](int64_t e) { return __float_as_int(A.cost[e]); }, sk, sbits, bst, sbk);
     if (!done) {
         sc.arena.release(m);
         return graph_contract_sorted(t, sc, sm, A, map, map_max, bad);
     }
     prof_mark(t, sc, PH_CONTRACT_SORT);
-    // 3. runs of every bucket
-    int32_t mxhi = -1, lastb = -1;
-    for (int64_t b = t.rank(); b < nbk; b += t.size()) {
-        const int32_t s = bst[b], e = bst[b + 1];
-        int32_t k = 0;
-        for (int32_t p = s; p < e;) {
-            const int32_t hi = (int32_t)(sk[p] >> 32);
-            int32_t q = p + 1;
-            while (q < e && (int32_t)(sk[q] >> 32) == hi) ++q;
-            mxhi = hi > mxhi ? hi : mxhi;
-            const bool diag = hi == (int32_t)b;
+    // the new graph's slot, sized for at most n edges; it ends at the arena's
+    // end, so it lies within the old graph's slot (n is the old edge count)
+    Arena &ar = sc.arena;
+    const uint64_t bytes = (uint64_t)(n + 1) * 12 + 3 * 256;
+    const uint64_t top = (ar.cap - bytes) & ~uint64_t(255);
+    if (ar.failed || bytes > ar.cap || top < ar.lo) {
+        ar.failed = 1;
+        return out;
+    }
+    const uint64_t words = ((uint64_t)(n + 1) * 4 + 255) / 256 * 256;
+    Graph h;
+    h.row = reinterpret_cast<int32_t *>(ar.base + top);
+    h.col = reinterpret_cast<int32_t *>(ar.base + top + words);
+    h.cost = reinterpret_cast<float *>(ar.base + top + 2 * words);
+    // 3. heads of the runs: a scan counts (runs not self-loops) << 32 | 0;
+    //    the head's thread handles its run
+    auto head = [&](int64_t p) {
+        return p == 0 || sbk[p] != sbk[p - 1] || (sk[p] >> 32) != (sk[p - 1] >> 32);
+    };
+    const int64_t nk = team_scan<Team, int64_t>(
+        t, sc, sm, n,
+        [&](int64_t p) -> int64_t { return head(p) && (int32_t)(sk[p] >> 32) != sbk[p] ? 1 : 0; },
+        [&](int64_t p, int64_t k, int64_t v) {
+            if (!head(p)) return;
+            const int32_t b = sbk[p], hi = (int32_t)(sk[p] >> 32);
+            int64_t q = p + 1;
+            while (q < n && q - p <= 32 && sbk[q] == b && (int32_t)(sk[q] >> 32) == hi) ++q;
             if (q - p <= 32) {
-                const float v = rsum_serial(q - p, [&](int x) { return __int_as_float(sbits[p + x]); });
-                if (diag) {
-                    if (v < 0.0f) fl[0] = 1;
+                const int32_t len = (int32_t)(q - p);
+                const float sum = rsum_serial(len, [&](int x) { return __int_as_float(sbits[p + x]); });
+                if (v) {
+                    h.row[k] = b;
+                    h.col[k] = hi;
+                    h.cost[k] = sum;
                 } else {
-                    rcol[s + k] = hi;
-                    rcost[s + k] = v;
+                    atomicMax(&fl[2], hi);
+                    if (sum < 0.0f) fl[0] = 1;
                 }
             } else {
+                while (q < n && sbk[q] == b && (int32_t)(sk[q] >> 32) == hi) ++q;
                 const int32_t slot = atomicAdd(&fl[1], 1);
-                longq[slot] = make_int4(p, q, diag ? -1 : s + k, 0);
-                if (!diag) rcol[s + k] = hi;
+                longq[slot] = make_int4((int32_t)p, (int32_t)q, v ? (int32_t)k : -1, hi);
+                if (v) {
+                    h.row[k] = b;
+                    h.col[k] = hi;
+                } else {
+                    atomicMax(&fl[2], hi);
+                }
             }
-            if (!diag) ++k;
-            p = q;
-        }
-        cnt[b] = k;
-        if (e > s) lastb = (int32_t)b;
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        mxhi = max(mxhi, __shfl_xor_sync(FULL, mxhi, o));
-        lastb = max(lastb, __shfl_xor_sync(FULL, lastb, o));
-    }
-    if (lane_id() == 0) {
-        if (mxhi >= 0) atomicMax(&fl[2], mxhi);
-        if (lastb >= 0) atomicMax(&fl[3], lastb);
-    }
-    t.sync();
+        });
     const int32_t nl = uread(&fl[1]);
     for (int64_t w = team_warp(t); w < nl; w += team_nwarps(t)) {
         const int4 L = longq[w];
@@ -388,51 +392,23 @@ __device__ Graph graph_contract(const Team &t, Scratch &sc, char *sm, const Grap
             if (L.z < 0) {
                 if (v < 0.0f) fl[0] = 1;
             } else {
-                rcost[L.z] = v;
+                h.cost[L.z] = v;
             }
         }
     }
-    // 4. rows placed by a scan of the counts, edges written into the slot
-    const int64_t nk = team_scan<Team, int64_t>(
-        t, sc, sm, nbk, [&](int64_t b) -> int64_t { return cnt[b]; },
-        [&](int64_t b, int64_t pre, int64_t) { opos[b] = (int32_t)pre; });
-    *bad = uread(&fl[0]);
-    Arena &ar = sc.arena;
-    const uint64_t bytes = (uint64_t)(nk + 1) * 12 + 3 * 256;
-    const uint64_t top = (ar.cap - bytes) & ~uint64_t(255);
-    if (ar.failed || bytes > ar.cap || top < ar.lo) {
-        ar.failed = 1;
-        return out;
-    }
-    const uint64_t words = ((uint64_t)(nk + 1) * 4 + 255) / 256 * 256;
-    Graph h;
-    h.row = reinterpret_cast<int32_t *>(ar.base + top);
-    h.col = reinterpret_cast<int32_t *>(ar.base + top + words);
-    h.cost = reinterpret_cast<float *>(ar.base + top + 2 * words);
-    h.n = nk;
-    h.rows = uread(&fl[3]) + 1;
-    h.cols = uread(&fl[2]) + 1;
-    uint32_t mn = 0xffffffffu;
-    for (int64_t b = t.rank(); b < nbk; b += t.size()) {
-        const int32_t s = bst[b], o = opos[b], c = cnt[b];
-        for (int32_t k = 0; k < c; ++k) {
-            const float v = rcost[s + k];
-            h.row[o + k] = (int32_t)b;
-            h.col[o + k] = rcol[s + k];
-            h.cost[o + k] = v;
-            const uint32_t f = float_ordered(v);
-            mn = f < mn ? f : mn;
-        }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        const uint32_t x = __shfl_xor_sync(FULL, mn, o);
-        mn = x < mn ? x : mn;
-    }
-    if (lane_id() == 0 && mn != 0xffffffffu) atomicMin(reinterpret_cast<unsigned *>(&fl[4]), mn);
     t.sync();
-    const uint32_t mo = (uint32_t)uread(&fl[4]);
-    h.cmin = nk > 0 ? __uint_as_float((mo & 0x80000000u) ? (mo & 0x7fffffffu) : ~mo) : unknown_cost();
+    *bad = uread(&fl[0]);
+    // 4. dims and the smallest cost (every new edge has row < col)
+    int32_t mc = -1;
+    float mn = 3.4e38f;
+    team_maxi_minf(
+        t, sc, sm, nk, -1, 3.4e38f, [&](int64_t e) { return h.col[e]; }, [&](int64_t e) { return h.cost[e]; }, mc,
+        mn);
+    const int32_t dmax = uread(&fl[2]);
+    h.n = nk;
+    h.rows = uread(&sbk[n - 1]) + 1;
+    h.cols = (mc > dmax ? mc : dmax) + 1;
+    h.cmin = nk > 0 ? mn : unknown_cost();
     ar.top = top;
     sc.arena.release(m);
     sc.alg_bytes += 20.0 * (double)n + 12.0 * (double)nk;

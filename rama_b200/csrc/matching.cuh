@@ -85,10 +85,12 @@ __device__ int32_t matching_contraction_map(const Team &t, Scratch &sc, char *sm
             // pick_best_neighbour: every live candidate offers itself to both
             // ends and stays a candidate for the next iteration.  A lane takes
             // MI edges at once (independent loads, gathers and atomics in
-            // flight together); a warp reserves list space once per 32 * MI.
+            // flight together); the CTA reserves list space for a tile of
+            // blockDim * MI edges with one atomic per list.
             constexpr int MI = 4;
-            auto offer_batch = [&](const int32_t (&u)[MI], const int32_t (&v)[MI], const uint32_t (&hb)[MI],
-                                   const bool (&live)[MI]) {
+            int32_t *wsum = reinterpret_cast<int32_t *>(sm);  // per warp: list count, touched count; then bases
+            auto offer_tile = [&](const int32_t (&u)[MI], const int32_t (&v)[MI], const uint32_t (&hb)[MI],
+                                  const bool (&live)[MI]) {
                 bool fu[MI], fv[MI];
 #pragma unroll
                 for (int k = 0; k < MI; ++k) {
@@ -105,18 +107,28 @@ __device__ int32_t matching_contraction_map(const Team &t, Scratch &sc, char *sm
                     nl += live[k];
                     nt += fu[k] + fv[k];
                 }
-                // one reservation per warp for both lists: lane prefixes by
-                // a warp scan of (touched << 16 | list) counts
+                // lane prefixes by a warp scan of (touched << 16 | list)
                 const int packed = (nt << 16) | nl;
                 const int incl = warp_incl_scan(packed);
-                const int tot = __shfl_sync(FULL, incl, 31);
-                int lbase = 0, tbase = 0;
-                if (lane_id() == 0) {
-                    if (tot & 0xffff) lbase = atomicAdd(&cnt_next[0], tot & 0xffff);
-                    if (tot >> 16) tbase = atomicAdd(&cnt_next[1], tot >> 16);
+                const int w = warp_in_block(), nw = blockDim.x >> 5;
+                if (lane_id() == 31) wsum[w] = incl;
+                __syncthreads();
+                if (threadIdx.x == 0) {
+                    int tl = 0, tt = 0;
+                    for (int q = 0; q < nw; ++q) {
+                        const int x = wsum[q];
+                        wsum[32 + q] = tl;
+                        wsum[64 + q] = tt;
+                        tl += x & 0xffff;
+                        tt += x >> 16;
+                    }
+                    wsum[96] = tl ? atomicAdd(&cnt_next[0], tl) : 0;
+                    wsum[97] = tt ? atomicAdd(&cnt_next[1], tt) : 0;
                 }
-                lbase = __shfl_sync(FULL, lbase, 0) + ((incl - packed) & 0xffff);
-                tbase = __shfl_sync(FULL, tbase, 0) + ((incl - packed) >> 16);
+                __syncthreads();
+                int lbase = wsum[96] + wsum[32 + w] + ((incl - packed) & 0xffff);
+                int tbase = wsum[97] + wsum[64 + w] + ((incl - packed) >> 16);
+                __syncthreads();  // wsum is rewritten by the next tile
 #pragma unroll
                 for (int k = 0; k < MI; ++k) {
                     if (live[k]) {
@@ -128,21 +140,24 @@ __device__ int32_t matching_contraction_map(const Team &t, Scratch &sc, char *sm
                     if (fv[k]) touched[cur][tbase++] = v[k];
                 }
             };
-            const int64_t stride = (int64_t)team_nwarps(t) * 32 * MI;
+            // block-uniform loops over tiles (every thread takes part in the
+            // tile's reservation)
+            const int64_t TILE = (int64_t)blockDim.x * MI;
+            const int64_t wofs = (int64_t)warp_in_block() * 32 * MI;
             if (it == 0) {
-                for (int64_t base = (int64_t)team_warp(t) * 32 * MI; base < A.n; base += stride) {
+                for (int64_t tile = (int64_t)t.block() * TILE; tile < A.n; tile += (int64_t)t.nblocks() * TILE) {
                     int32_t u[MI], v[MI];
                     uint32_t hb[MI];
                     bool live[MI];
                     float c[MI];
 #pragma unroll
                     for (int k = 0; k < MI; ++k) {
-                        const int64_t e = base + k * 32 + lane_id();
+                        const int64_t e = tile + wofs + k * 32 + lane_id();
                         c[k] = e < A.n ? A.cost[e] : 0.0f;
                     }
 #pragma unroll
                     for (int k = 0; k < MI; ++k) {
-                        const int64_t e = base + k * 32 + lane_id();
+                        const int64_t e = tile + wofs + k * 32 + lane_id();
                         live[k] = e < A.n && c[k] > thresh;
                         u[k] = live[k] ? A.row[e] : 0;
                         v[k] = live[k] ? A.col[e] : 0;
@@ -150,18 +165,18 @@ __device__ int32_t matching_contraction_map(const Team &t, Scratch &sc, char *sm
                     }
 #pragma unroll
                     for (int k = 0; k < MI; ++k) live[k] = live[k] && u[k] != v[k];
-                    offer_batch(u, v, hb, live);
+                    offer_tile(u, v, hb, live);
                 }
             } else {
                 const int2 *L = cand[cur];
                 const uint32_t *LB = cbits[cur];
-                for (int64_t base = (int64_t)team_warp(t) * 32 * MI; base < ncand; base += stride) {
+                for (int64_t tile = (int64_t)t.block() * TILE; tile < ncand; tile += (int64_t)t.nblocks() * TILE) {
                     int32_t u[MI], v[MI];
                     uint32_t hb[MI];
                     bool live[MI];
 #pragma unroll
                     for (int k = 0; k < MI; ++k) {
-                        const int64_t q = base + k * 32 + lane_id();
+                        const int64_t q = tile + wofs + k * 32 + lane_id();
                         int2 uv = make_int2(0, 0);
                         hb[k] = 0;
                         if (q < ncand) {
@@ -180,7 +195,7 @@ __device__ int32_t matching_contraction_map(const Team &t, Scratch &sc, char *sm
                     }
 #pragma unroll
                     for (int k = 0; k < MI; ++k) live[k] = live[k] && !mu[k] && !mv[k];
-                    offer_batch(u, v, hb, live);
+                    offer_tile(u, v, hb, live);
                 }
             }
             if (t.rank() < 2) cnt_clear[t.rank()] = 0;  // counters of the iteration after next

@@ -863,11 +863,12 @@ __device__ __forceinline__ void smem_bitonic(uint64_t *key, int32_t *idx, int m,
 // The general form: the slot pass calls bk_slot(i) once per item (it may
 // store what it computes for the scatter pass), the scatter pass calls
 // bucket(i), sub(i) and pay(i); idx_out receives pay(i) of each item instead of
-// its index (team_bucket_sort below: pay(i) = i).
+// its index (team_bucket_sort below: pay(i) = i), and bucket_out, if given, the
+// bucket of each sorted position.
 template <class Team, class BkSlot, class Bk, class Sub, class Pay>
 __device__ bool team_bucket_sort_ex(const Team &t, Scratch &sc, char *sm, int64_t n, int32_t nb, BkSlot bk_slot,
                                     Bk bucket, Sub sub, Pay pay, uint64_t *keys_out, int32_t *idx_out,
-                                    int32_t *bstart)
+                                    int32_t *bstart, int32_t *bucket_out = nullptr)
 {
     uint64_t am = sc.arena.mark();
     int32_t *slot = sc.arena.take<int32_t>(n + 1);
@@ -894,22 +895,23 @@ __device__ bool team_bucket_sort_ex(const Team &t, Scratch &sc, char *sm, int64_
         if (valid) slot[i] = s0 + __popc(peers & lanemask_lt());
     }
     t.sync();
-    const int32_t big = team_max<Team, int32_t>(t, sc, sm, nb, 0, [&](int64_t b) { return bstart[b]; });
-    if (big > BUCKET_MAX) {
+    // bucket starts; buckets of more than 64 items go to the warp and CTA
+    // lists (any order); one of more than BUCKET_MAX ends the sort
+    team_scan<Team, int64_t>(
+        t, sc, sm, nb, [&](int64_t b) -> int64_t { return bstart[b]; },
+        [&](int64_t b, int64_t pre, int64_t c) {
+            bstart[b] = (int32_t)pre;
+            if (c > BUCKET_MAX)
+                nlist[2] = 1;
+            else if (c > 256)
+                clist[atomicAdd(&nlist[1], 1)] = (int32_t)b;
+            else if (c > 64)
+                wlist[atomicAdd(&nlist[0], 1)] = (int32_t)b;
+        });
+    if (uread(&nlist[2])) {
         sc.arena.release(am);
         return false;
     }
-    // buckets of more than 64 items: the warp and CTA lists (any order)
-    for (int64_t b = t.rank(); b < nb; b += t.size()) {
-        const int32_t c = bstart[b];
-        if (c > 256)
-            clist[atomicAdd(&nlist[1], 1)] = (int32_t)b;
-        else if (c > 64)
-            wlist[atomicAdd(&nlist[0], 1)] = (int32_t)b;
-    }
-    team_scan<Team, int64_t>(
-        t, sc, sm, nb, [&](int64_t b) -> int64_t { return bstart[b]; },
-        [&](int64_t b, int64_t pre, int64_t) { bstart[b] = (int32_t)pre; });
     if (t.rank() == 0) bstart[nb] = (int32_t)n;
     t.sync();
     for (int64_t i = t.rank(); i < n; i += t.size()) {
@@ -927,6 +929,7 @@ __device__ bool team_bucket_sort_ex(const Team &t, Scratch &sc, char *sm, int64_
         if (e - s > 64) {
             keys_out[p] = tk[p];
             idx_out[p] = ti[p];
+            if (bucket_out) bucket_out[p] = b;
             continue;
         }
         const uint64_t k = tk[p];
@@ -937,6 +940,7 @@ __device__ bool team_bucket_sort_ex(const Team &t, Scratch &sc, char *sm, int64_
         }
         keys_out[s + r] = k;
         idx_out[s + r] = ti[p];
+        if (bucket_out) bucket_out[s + r] = b;
     }
     t.sync();
     // 65..256 items: a warp, bitonic in its share of the staging area
