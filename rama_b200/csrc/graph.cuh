@@ -328,12 +328,11 @@ __device__ Graph graph_contract(const Team &t, Scratch &sc, char *sm, const Grap
         },
         [&](int64_t e) { return lohi[e].x; },
         [&](int64_t e) -> uint64_t { return ((uint64_t)(uint32_t)lohi[e].y << 32) | (uint64_t)e; },
-        [&](int64_t e) { return __float_as_int(A.cost[e]); }, sk, sbits, bst, sbk);
+        [&](int64_t e) { return __float_as_int(A.cost[e]); }, sk, sbits, bst, sbk, PH_CSORT_SLOT);
     if (!done) {
         sc.arena.release(m);
         return graph_contract_sorted(t, sc, sm, A, map, map_max, bad);
     }
-    prof_mark(t, sc, PH_CONTRACT_SORT);
     // the new graph's slot, sized for at most n edges; it ends at the arena's
     // end, so it lies within the old graph's slot (n is the old edge count)
     Arena &ar = sc.arena;
@@ -343,6 +342,7 @@ __device__ Graph graph_contract(const Team &t, Scratch &sc, char *sm, const Grap
         ar.failed = 1;
         return out;
     }
+    prof_mark(t, sc, PH_CONTRACT_SORT);
     const uint64_t words = ((uint64_t)(n + 1) * 4 + 255) / 256 * 256;
     Graph h;
     h.row = reinterpret_cast<int32_t *>(ar.base + top);
@@ -363,7 +363,10 @@ __device__ Graph graph_contract(const Team &t, Scratch &sc, char *sm, const Grap
             while (q < n && q - p <= 32 && sbk[q] == b && (int32_t)(sk[q] >> 32) == hi) ++q;
             if (q - p <= 32) {
                 const int32_t len = (int32_t)(q - p);
-                const float sum = rsum_serial(len, [&](int x) { return __int_as_float(sbits[p + x]); });
+                const float sum =
+                    len <= RSUM_THREAD_MAX
+                        ? rsum_upto8(reinterpret_cast<const float *>(sbits + p), len)
+                        : rsum_serial(len, [&](int x) { return __int_as_float(sbits[p + x]); });
                 if (v) {
                     h.row[k] = b;
                     h.col[k] = hi;
@@ -397,6 +400,7 @@ __device__ Graph graph_contract(const Team &t, Scratch &sc, char *sm, const Grap
         }
     }
     t.sync();
+    prof_mark(t, sc, PH_CONTRACT_RUNS);
     *bad = uread(&fl[0]);
     // 4. dims and the smallest cost (every new edge has row < col)
     int32_t mc = -1;

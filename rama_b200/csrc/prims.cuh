@@ -80,6 +80,10 @@ enum Phase : int {
     PH_MATCH_ITER = 9,    // the offer / match iterations of a matching round
     PH_CONTRACT_SORT = 10,  // the bucket sort of a contraction
     PH_CSR = 11,          // symmetric CSR builds (cycle search, forest)
+    PH_CSORT_SLOT = 12,   // contraction sort: endpoints and bucket slots
+    PH_CSORT_SCATTER = 13,  // ... bucket starts and the scatter
+    PH_CSORT_RANK = 14,   // ... ordering within the buckets
+    PH_CONTRACT_RUNS = 15,  // contraction: run heads, sums, the new edges
     PH_COUNT = 16
 };
 
@@ -868,7 +872,7 @@ __device__ __forceinline__ void smem_bitonic(uint64_t *key, int32_t *idx, int m,
 template <class Team, class BkSlot, class Bk, class Sub, class Pay>
 __device__ bool team_bucket_sort_ex(const Team &t, Scratch &sc, char *sm, int64_t n, int32_t nb, BkSlot bk_slot,
                                     Bk bucket, Sub sub, Pay pay, uint64_t *keys_out, int32_t *idx_out,
-                                    int32_t *bstart, int32_t *bucket_out = nullptr)
+                                    int32_t *bstart, int32_t *bucket_out = nullptr, int detail_phase = -1)
 {
     uint64_t am = sc.arena.mark();
     int32_t *slot = sc.arena.take<int32_t>(n + 1);
@@ -895,6 +899,7 @@ __device__ bool team_bucket_sort_ex(const Team &t, Scratch &sc, char *sm, int64_
         if (valid) slot[i] = s0 + __popc(peers & lanemask_lt());
     }
     t.sync();
+    if (detail_phase >= 0) prof_mark(t, sc, detail_phase);
     // bucket starts; buckets of more than 64 items go to the warp and CTA
     // lists (any order); one of more than BUCKET_MAX ends the sort
     team_scan<Team, int64_t>(
@@ -922,6 +927,7 @@ __device__ bool team_bucket_sort_ex(const Team &t, Scratch &sc, char *sm, int64_
         tb[p] = b;
     }
     t.sync();
+    if (detail_phase >= 0) prof_mark(t, sc, detail_phase + 1);
     // up to 64 items: each item's rank in its bucket is the number of smaller
     // keys there (neighbouring threads read the same bucket)
     for (int64_t p = t.rank(); p < n; p += t.size()) {
@@ -994,6 +1000,7 @@ __device__ bool team_bucket_sort_ex(const Team &t, Scratch &sc, char *sm, int64_
         }
     }
     t.sync();
+    if (detail_phase >= 0) prof_mark(t, sc, detail_phase + 2);
     sc.arena.release(am);
     return true;
 }
