@@ -17,6 +17,7 @@ struct TriBuf {
     int64_t budget;
     int64_t count;  // the reference's triangle counter (budget+1 once overflowed)
     int64_t num;    // valid entries: min(count, budget)
+    int none;       // no repulsive edge has an attractive edge at both ends: no cycle of any length
 };
 
 __device__ __forceinline__ int count_common(const int32_t *adj, int32_t a0, int32_t a1, int32_t b0, int32_t b1)
@@ -249,6 +250,7 @@ __device__ void conflicted_cycles(const Team &t, Scratch &sc, char *sm, const Gr
     tb.count = 0;
     tb.num = 0;
     tb.budget = 0;
+    tb.none = 0;
     tb.t1 = tb.t2 = tb.t3 = nullptr;
     if (max_len < 3 || A.n == 0) return;
     // the smallest cost: known from the pass that built the graph, or one pass
@@ -285,7 +287,10 @@ __device__ void conflicted_cycles(const Team &t, Scratch &sc, char *sm, const Gr
     const int64_t Rall = packed & 0xffffffffll;
     const int64_t R = packed >> 32;
     sc.alg_bytes += 12.0 * (double)A.n;
-    if (P == 0 || R == 0) return;
+    if (P == 0 || R == 0) {
+        tb.none = 1;
+        return;
+    }
     team_scan<Team, int64_t>(
         t, sc, sm, A.n, [&](int64_t e) -> int64_t { return rep_code(e) >> 32; },
         [&](int64_t e, int64_t pre, int64_t v) {

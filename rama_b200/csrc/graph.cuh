@@ -89,9 +89,77 @@ __device__ __forceinline__ uint64_t pack_key(int32_t a, int32_t b, int nbits)
 
 // dCOO ctor with unsorted input (src/dCOO.cu:38-45): endpoints ordered,
 // sorted by (row,col), stable.  Inputs are (i, j, c) of length n.
+// By buckets of the smaller endpoint: the bucket sort orders each bucket by
+// (larger endpoint, edge index) and carries the cost bits and the bucket
+// along, and the sorted edges are written straight into the graph slot.
+// Buckets of more than BUCKET_MAX edges go through a stable radix sort of
+// their packed (min, max) keys inside the bucket sort; edge lists of 2^31 or
+// more take graph_from_edges_sorted (one radix sort of every edge's keys).
+template <class Team>
+__device__ Graph graph_from_edges_sorted(const Team &t, Scratch &sc, char *sm, const int32_t *i, const int32_t *j,
+                                         const float *c, int64_t n);
+
 template <class Team>
 __device__ Graph graph_from_edges(const Team &t, Scratch &sc, char *sm, const int32_t *i, const int32_t *j,
                                   const float *c, int64_t n)
+{
+    if (n == 0 || n >= (int64_t(1) << 31)) return graph_from_edges_sorted(t, sc, sm, i, j, c, n);
+    Graph out;
+    out.n = n;
+    out.rows = out.cols = 0;
+    out.cmin = unknown_cost();
+    const int32_t mx = team_max<Team, int32_t>(t, sc, sm, n, 0, [&](int64_t e) { return i[e] > j[e] ? i[e] : j[e]; });
+    const int nbh = bits_for((uint64_t)(mx > 0 ? mx : 1));
+    uint64_t m = sc.arena.mark();
+    int2 *lohi = sc.arena.take<int2>(n + 1);
+    uint64_t *sk = sc.arena.take<uint64_t>(n + 1);
+    int32_t *sbits = sc.arena.take<int32_t>(n + 1);
+    int32_t *sbk = sc.arena.take<int32_t>(n + 1);
+    int32_t *bst = sc.arena.take<int32_t>((int64_t)mx + 2);
+    if (!sc.arena.ok()) return out;
+    const bool done = team_bucket_sort_ex(
+        t, sc, sm, n, mx + 1,
+        [&](int64_t e) {
+            const int32_t a = i[e], b = j[e];
+            const int32_t lo = a < b ? a : b, hi = a < b ? b : a;
+            lohi[e] = make_int2(lo, hi);
+            return lo;
+        },
+        [&](int64_t e) { return lohi[e].x; },
+        [&](int64_t e) -> uint64_t { return ((uint64_t)(uint32_t)lohi[e].y << 32) | (uint64_t)e; },
+        [&](int64_t e) { return __float_as_int(c[e]); }, sk, sbits, bst, sbk, -1,
+        [&](int64_t e) -> uint64_t { return ((uint64_t)(uint32_t)lohi[e].x << nbh) | (uint32_t)lohi[e].y; },
+        2 * nbh);
+    if (!done) return out;
+    Arena &ar = sc.arena;
+    const uint64_t bytes = (uint64_t)(n + 1) * 12 + 3 * 256;
+    const uint64_t top = (ar.cap - bytes) & ~uint64_t(255);
+    if (ar.failed || bytes > ar.cap || top < ar.lo) {
+        ar.failed = 1;
+        return out;
+    }
+    const uint64_t words = ((uint64_t)(n + 1) * 4 + 255) / 256 * 256;
+    Graph g;
+    g.row = reinterpret_cast<int32_t *>(ar.base + top);
+    g.col = reinterpret_cast<int32_t *>(ar.base + top + words);
+    g.cost = reinterpret_cast<float *>(ar.base + top + 2 * words);
+    g.n = n;
+    for (int64_t p = t.rank(); p < n; p += t.size()) {
+        g.row[p] = sbk[p];
+        g.col[p] = (int32_t)(sk[p] >> 32);
+        g.cost[p] = __int_as_float(sbits[p]);
+    }
+    t.sync();
+    graph_set_dims(t, sc, sm, g);
+    ar.top = top;
+    sc.arena.release(m);
+    sc.alg_bytes += 24.0 * (double)n;
+    return g;
+}
+
+template <class Team>
+__device__ Graph graph_from_edges_sorted(const Team &t, Scratch &sc, char *sm, const int32_t *i, const int32_t *j,
+                                         const float *c, int64_t n)
 {
     Graph out;
     out.n = n;
@@ -292,9 +360,10 @@ __device__ Graph graph_contract_sorted(const Team &t, Scratch &sc, char *sm, con
 //   4. one pass over the new edges gives the largest column and the smallest
 //      cost; the rows are the last bucket + 1 (dims are taken before the
 //      diagonal goes, as the reference does).
-// A bucket of more than BUCKET_MAX edges sends the contraction to
-// graph_contract_sorted (one radix sort of the packed keys).  Both give the
-// same graph bit for bit.
+// Buckets of more than BUCKET_MAX edges are sorted by a stable radix sort of
+// their packed (lo, hi) keys inside the bucket sort; graph_contract_sorted
+// (one radix sort of every edge's packed keys) remains for edge lists of
+// 2^31 edges or more.  Both give the same graph bit for bit.
 template <class Team>
 __device__ Graph graph_contract(const Team &t, Scratch &sc, char *sm, const Graph &A, const int32_t *map,
                                 int32_t map_max, int *bad)
@@ -303,6 +372,7 @@ __device__ Graph graph_contract(const Team &t, Scratch &sc, char *sm, const Grap
     Graph out = A;
     if (n == 0 || n >= (int64_t(1) << 31)) return graph_contract_sorted(t, sc, sm, A, map, map_max, bad);
     const int32_t nbk = map_max + 1;
+    const int nbh = bits_for((uint64_t)(map_max > 0 ? map_max : 1));
     uint64_t m = sc.arena.mark();
     int2 *lohi = sc.arena.take<int2>(n + 1);
     uint64_t *sk = sc.arena.take<uint64_t>(n + 1);
@@ -328,7 +398,9 @@ __device__ Graph graph_contract(const Team &t, Scratch &sc, char *sm, const Grap
         },
         [&](int64_t e) { return lohi[e].x; },
         [&](int64_t e) -> uint64_t { return ((uint64_t)(uint32_t)lohi[e].y << 32) | (uint64_t)e; },
-        [&](int64_t e) { return __float_as_int(A.cost[e]); }, sk, sbits, bst, sbk, PH_CSORT_SLOT);
+        [&](int64_t e) { return __float_as_int(A.cost[e]); }, sk, sbits, bst, sbk, PH_CSORT_SLOT,
+        [&](int64_t e) -> uint64_t { return ((uint64_t)(uint32_t)lohi[e].x << nbh) | (uint32_t)lohi[e].y; },
+        2 * nbh);
     if (!done) {
         sc.arena.release(m);
         return graph_contract_sorted(t, sc, sm, A, map, map_max, bad);

@@ -346,7 +346,8 @@ __device__ void mp_iteration(const Team &t, const Mp &mp)
 // in the top slot is replaced by the reparametrised one.
 template <class Team>
 __device__ double dual_update_cycle_length(const Team &t, Scratch &sc, char *sm, Graph &A, int c, int num_iter,
-                                           float tri_factor, float tol, int64_t *num_tri, bool *failed)
+                                           float tri_factor, float tol, int64_t *num_tri, bool *failed,
+                                           bool *no_cycles)
 {
     uint64_t m = sc.arena.mark();
     TriBuf tb;
@@ -359,6 +360,7 @@ __device__ double dual_update_cycle_length(const Team &t, Scratch &sc, char *sm,
         return 0.0;
     }
     *num_tri = tb.count;
+    *no_cycles = tb.none != 0;
     if (tb.count == 0) {
         sc.arena.release(m);
         return graph_lb(t, sc, A);
@@ -408,13 +410,17 @@ __device__ double dual_solver(const Team &t, Scratch &sc, char *sm, Graph &A, in
     int64_t nt = 0;
     for (int o = 0; o < num_outer; ++o) {
         for (int c = 3; c <= max_len; ++c) {
-            bool failed = false;
-            fin = dual_update_cycle_length(t, sc, sm, A, c, num_iter, tri_factor, tol, &nt, &failed);
+            bool failed = false, none = false;
+            fin = dual_update_cycle_length(t, sc, sm, A, c, num_iter, tri_factor, tol, &nt, &failed, &none);
             if (failed) {
                 sc.arena.failed = 0;
                 if (oom) *oom = 1;
                 return graph_lb(t, sc, A);
             }
+            // the graph is unchanged and no repulsive edge can close a cycle:
+            // the longer cycle lengths find nothing either (nt == 0 ends the
+            // outer loop too)
+            if (none) break;
         }
         if (nt == 0 || (o > 0 && (fin - prev) < 1e-3)) break;
         prev = fin;

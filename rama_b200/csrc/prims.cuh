@@ -869,10 +869,22 @@ __device__ __forceinline__ void smem_bitonic(uint64_t *key, int32_t *idx, int m,
 // bucket(i), sub(i) and pay(i); idx_out receives pay(i) of each item instead of
 // its index (team_bucket_sort below: pay(i) = i), and bucket_out, if given, the
 // bucket of each sorted position.
-template <class Team, class BkSlot, class Bk, class Sub, class Pay>
+//
+// Buckets of more than BUCKET_MAX items: with big_bits > 0 their items are
+// taken out in input order and sorted by a stable LSD radix sort of
+// big_key(i) (big_bits bits), which must order them as (bucket, sub) does
+// once equal keys keep their input order -- e.g. (bucket, hi) when sub is
+// (hi, item index).  With big_bits == 0 such a bucket makes the sort return
+// false.
+struct NoBigKey {
+    __device__ uint64_t operator()(int64_t) const { return 0; }
+};
+
+template <class Team, class BkSlot, class Bk, class Sub, class Pay, class BigKey = NoBigKey>
 __device__ bool team_bucket_sort_ex(const Team &t, Scratch &sc, char *sm, int64_t n, int32_t nb, BkSlot bk_slot,
                                     Bk bucket, Sub sub, Pay pay, uint64_t *keys_out, int32_t *idx_out,
-                                    int32_t *bstart, int32_t *bucket_out = nullptr, int detail_phase = -1)
+                                    int32_t *bstart, int32_t *bucket_out = nullptr, int detail_phase = -1,
+                                    BigKey big_key = BigKey(), int big_bits = 0)
 {
     uint64_t am = sc.arena.mark();
     int32_t *slot = sc.arena.take<int32_t>(n + 1);
@@ -913,7 +925,8 @@ __device__ bool team_bucket_sort_ex(const Team &t, Scratch &sc, char *sm, int64_
             else if (c > 64)
                 wlist[atomicAdd(&nlist[0], 1)] = (int32_t)b;
         });
-    if (uread(&nlist[2])) {
+    const bool has_big = uread(&nlist[2]) != 0;
+    if (has_big && big_bits <= 0) {
         sc.arena.release(am);
         return false;
     }
@@ -933,9 +946,11 @@ __device__ bool team_bucket_sort_ex(const Team &t, Scratch &sc, char *sm, int64_
     for (int64_t p = t.rank(); p < n; p += t.size()) {
         const int32_t b = tb[p], s = bstart[b], e = bstart[b + 1];
         if (e - s > 64) {
-            keys_out[p] = tk[p];
-            idx_out[p] = ti[p];
-            if (bucket_out) bucket_out[p] = b;
+            if (e - s <= BUCKET_MAX) {
+                keys_out[p] = tk[p];
+                idx_out[p] = ti[p];
+                if (bucket_out) bucket_out[p] = b;
+            }
             continue;
         }
         const uint64_t k = tk[p];
@@ -1000,6 +1015,44 @@ __device__ bool team_bucket_sort_ex(const Team &t, Scratch &sc, char *sm, int64_
         }
     }
     t.sync();
+    if (has_big) {
+        // the buckets beyond BUCKET_MAX: their items in input order, a stable
+        // radix sort of big_key, then each into its bucket's range
+        auto bsize = [&](int64_t i) {
+            const int32_t b = (int32_t)bucket(i);
+            return bstart[b + 1] - bstart[b];
+        };
+        uint64_t bm = sc.arena.mark();
+        const int64_t nbig = team_sum<Team, int64_t>(t, sc, sm, n, [&](int64_t i) -> int64_t {
+            return bsize(i) > BUCKET_MAX ? 1 : 0;
+        });
+        uint64_t *bk1 = sc.arena.take<uint64_t>(nbig + 1), *bk2 = sc.arena.take<uint64_t>(nbig + 1);
+        int32_t *bv1 = sc.arena.take<int32_t>(nbig + 1), *bv2 = sc.arena.take<int32_t>(nbig + 1);
+        int32_t *kfirst = sc.arena.take<int32_t>((int64_t)nb + 1);
+        if (!sc.arena.ok()) return false;
+        team_compact(
+            t, sc, sm, n, [&](int64_t i) { return bsize(i) > BUCKET_MAX; },
+            [&](int64_t i, int64_t k) {
+                bk1[k] = big_key(i);
+                bv1[k] = (int32_t)i;
+            });
+        team_sort_pairs(t, sc, sm, bk1, bv1, bk2, bv2, nbig, big_bits);
+        for (int64_t k = t.rank(); k < nbig; k += t.size()) {
+            const int32_t b = (int32_t)bucket(bv1[k]);
+            if (k == 0 || (int32_t)bucket(bv1[k - 1]) != b) kfirst[b] = (int32_t)k;
+        }
+        t.sync();
+        for (int64_t k = t.rank(); k < nbig; k += t.size()) {
+            const int64_t i = bv1[k];
+            const int32_t b = (int32_t)bucket(i);
+            const int64_t p = (int64_t)bstart[b] + (k - kfirst[b]);
+            keys_out[p] = sub(i);
+            idx_out[p] = pay(i);
+            if (bucket_out) bucket_out[p] = b;
+        }
+        t.sync();
+        sc.arena.release(bm);
+    }
     if (detail_phase >= 0) prof_mark(t, sc, detail_phase + 2);
     sc.arena.release(am);
     return true;
