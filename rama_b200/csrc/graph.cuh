@@ -420,16 +420,25 @@ __device__ Graph graph_contract(const Team &t, Scratch &sc, char *sm, const Grap
     h.row = reinterpret_cast<int32_t *>(ar.base + top);
     h.col = reinterpret_cast<int32_t *>(ar.base + top + words);
     h.cost = reinterpret_cast<float *>(ar.base + top + 2 * words);
-    // 3. heads of the runs: a scan counts (runs not self-loops) << 32 | 0;
-    //    the head's thread handles its run
+    // 3. heads of the runs: one scan counts every run (high 32 bits) and the
+    //    runs that are not self-loops (low 32 bits); the head's thread sums a
+    //    run of at most 32 edges, a longer run goes to a warp, which finds its
+    //    end at the next run's head
     auto head = [&](int64_t p) {
         return p == 0 || sbk[p] != sbk[p - 1] || (sk[p] >> 32) != (sk[p - 1] >> 32);
     };
-    const int64_t nk = team_scan<Team, int64_t>(
+    int32_t *runstart = reinterpret_cast<int32_t *>(lohi);  // lohi is dead after the sort
+    const int64_t packed = team_scan<Team, int64_t>(
         t, sc, sm, n,
-        [&](int64_t p) -> int64_t { return head(p) && (int32_t)(sk[p] >> 32) != sbk[p] ? 1 : 0; },
-        [&](int64_t p, int64_t k, int64_t v) {
-            if (!head(p)) return;
+        [&](int64_t p) -> int64_t {
+            if (!head(p)) return 0;
+            return (int64_t(1) << 32) | ((int32_t)(sk[p] >> 32) != sbk[p] ? 1 : 0);
+        },
+        [&](int64_t p, int64_t pre, int64_t v) {
+            if (!v) return;
+            const int64_t k = pre & 0xffffffffll, r = pre >> 32;
+            const bool nondiag = (v & 1) != 0;
+            runstart[r] = (int32_t)p;
             const int32_t b = sbk[p], hi = (int32_t)(sk[p] >> 32);
             int64_t q = p + 1;
             while (q < n && q - p <= 32 && sbk[q] == b && (int32_t)(sk[q] >> 32) == hi) ++q;
@@ -439,7 +448,7 @@ __device__ Graph graph_contract(const Team &t, Scratch &sc, char *sm, const Grap
                     len <= RSUM_THREAD_MAX
                         ? rsum_upto8(reinterpret_cast<const float *>(sbits + p), len)
                         : rsum_serial(len, [&](int x) { return __int_as_float(sbits[p + x]); });
-                if (v) {
+                if (nondiag) {
                     h.row[k] = b;
                     h.col[k] = hi;
                     h.cost[k] = sum;
@@ -448,10 +457,9 @@ __device__ Graph graph_contract(const Team &t, Scratch &sc, char *sm, const Grap
                     if (sum < 0.0f) fl[0] = 1;
                 }
             } else {
-                while (q < n && sbk[q] == b && (int32_t)(sk[q] >> 32) == hi) ++q;
                 const int32_t slot = atomicAdd(&fl[1], 1);
-                longq[slot] = make_int4((int32_t)p, (int32_t)q, v ? (int32_t)k : -1, hi);
-                if (v) {
+                longq[slot] = make_int4((int32_t)p, (int32_t)r, nondiag ? (int32_t)k : -1, hi);
+                if (nondiag) {
                     h.row[k] = b;
                     h.col[k] = hi;
                 } else {
@@ -459,10 +467,12 @@ __device__ Graph graph_contract(const Team &t, Scratch &sc, char *sm, const Grap
                 }
             }
         });
+    const int64_t nk = packed & 0xffffffffll, nruns = packed >> 32;
     const int32_t nl = uread(&fl[1]);
     for (int64_t w = team_warp(t); w < nl; w += team_nwarps(t)) {
         const int4 L = longq[w];
-        const float v = rsum_warp(L.y - L.x, [&](int64_t x) { return __int_as_float(sbits[L.x + x]); });
+        const int64_t end = L.y + 1 < nruns ? (int64_t)runstart[L.y + 1] : n;
+        const float v = rsum_warp(end - L.x, [&](int64_t x) { return __int_as_float(sbits[L.x + x]); });
         if (lane_id() == 0) {
             if (L.z < 0) {
                 if (v < 0.0f) fl[0] = 1;

@@ -1015,7 +1015,8 @@ __device__ bool team_bucket_sort_ex(const Team &t, Scratch &sc, char *sm, int64_
         }
     }
     t.sync();
-    if (has_big) {
+    // (compiled only for callers that give a big key)
+    if constexpr (!std::is_same<BigKey, NoBigKey>::value) if (has_big) {
         // the buckets beyond BUCKET_MAX: their items in input order, a stable
         // radix sort of big_key, then each into its bucket's range
         auto bsize = [&](int64_t i) {
