@@ -90,8 +90,8 @@ typedef struct {
     double phase_ms[16];     /* time per phase: init, cycle search, MP build, MP iterations + bound,
                                 dual commit, matching (threshold, labels), forest contraction set,
                                 contraction (after its sort), other, matching iterations, contraction
-                                sort (set-up), CSR builds, contraction sort (endpoints and slots,
-                                scatter, ordering in buckets), contraction runs */
+                                sort of buckets beyond 4096 edges, CSR builds, contraction sort
+                                (endpoints and slots, scatter, ordering in buckets), contraction runs */
     double phase_bytes[16];  /* algorithmic bytes per phase (same order), the parts of alg_bytes */
 } rama_stats;
 

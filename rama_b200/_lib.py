@@ -77,7 +77,7 @@ class RamaTuning(C.Structure):
 
 
 PHASES = ("init", "cycles", "mp_build", "mp_iter", "dual_commit", "matching", "woc", "contract", "other",
-          "match_iter", "contract_sort", "csr", "csort_slot", "csort_scatter", "csort_rank", "contract_runs")
+          "match_iter", "csort_big", "csr", "csort_slot", "csort_scatter", "csort_rank", "contract_runs")
 
 
 _P = C.c_void_p

@@ -414,7 +414,6 @@ __device__ Graph graph_contract(const Team &t, Scratch &sc, char *sm, const Grap
         ar.failed = 1;
         return out;
     }
-    prof_mark(t, sc, PH_CONTRACT_SORT);
     const uint64_t words = ((uint64_t)(n + 1) * 4 + 255) / 256 * 256;
     Graph h;
     h.row = reinterpret_cast<int32_t *>(ar.base + top);

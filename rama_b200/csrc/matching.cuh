@@ -38,7 +38,7 @@ __device__ int32_t matching_contraction_map(const Team &t, Scratch &sc, char *sm
     unsigned long long *offer[2];
     offer[0] = sc.arena.take<unsigned long long>((int64_t)M + 1);
     offer[1] = sc.arena.take<unsigned long long>((int64_t)M + 1);
-    int32_t *flags = sc.arena.take<int32_t>(64);  // [it]: matched a pair; [16 + 2k]: list sizes
+    int32_t *flags = sc.arena.take<int32_t>(64);  // [16 + 4k]: list sizes and new pairs of iteration k
     if (!sc.arena.ok()) return 0;
     for (int64_t v = t.rank(); v < M; v += t.size()) {
         nm[v] = (int32_t)v;
@@ -49,11 +49,14 @@ __device__ int32_t matching_contraction_map(const Team &t, Scratch &sc, char *sm
     if (t.rank() < 64) flags[t.rank()] = 0;
     // determine_matching_threshold (:76-86): mean of the non-negative costs
     // of the doubled edge list, CSUM over the directed list
-    const double S = team_csum(t, sc, A.n, [&](int64_t e) -> double {
-        float c = A.cost[e];
-        return c >= 0.0f ? (double)c : 0.0;
-    });
-    const int64_t K = team_sum<Team, int64_t>(t, sc, sm, A.n, [&](int64_t e) -> int64_t { return A.cost[e] >= 0.0f; });
+    int64_t K = 0;
+    const double S = team_csum_count(
+        t, sc, A.n,
+        [&](int64_t e) -> double {
+            float c = A.cost[e];
+            return c >= 0.0f ? (double)c : 0.0;
+        },
+        [&](int64_t e) { return A.cost[e] >= 0.0f; }, &K);
     int32_t prev = 0;
     if (K > 0) {
         const float sum_f = (float)(2.0 * S);
@@ -80,8 +83,8 @@ __device__ int32_t matching_contraction_map(const Team &t, Scratch &sc, char *sm
         for (int it = 0; it < 10; ++it) {
             const int cur = it & 1, nxt = cur ^ 1;
             unsigned long long *cur_offer = offer[cur], *next_offer = offer[nxt];
-            int32_t *cnt_next = flags + 16 + 2 * (it & 7);  // [0]: next list, [1]: touched
-            int32_t *cnt_clear = flags + 16 + 2 * ((it + 1) & 7);
+            int32_t *cnt_next = flags + 16 + 4 * (it & 7);  // [0]: next list, [1]: touched, [2]: pairs
+            int32_t *cnt_clear = flags + 16 + 4 * ((it + 1) & 7);
             // pick_best_neighbour: every live candidate offers itself to both
             // ends and stays a candidate for the next iteration.  A lane takes
             // MI edges at once (independent loads, gathers and atomics in
@@ -198,7 +201,7 @@ __device__ int32_t matching_contraction_map(const Team &t, Scratch &sc, char *sm
                     offer_tile(u, v, hb, live);
                 }
             }
-            if (t.rank() < 2) cnt_clear[t.rank()] = 0;  // counters of the iteration after next
+            if (t.rank() < 3) cnt_clear[t.rank()] = 0;  // counters of the next iteration
             t.sync();
             const int64_t nread = it == 0 ? A.n : ncand;
             const int32_t ntouch = uread(&cnt_next[1]);
@@ -208,39 +211,49 @@ __device__ int32_t matching_contraction_map(const Team &t, Scratch &sc, char *sm
             const int32_t *T0 = touched[cur];
             const int32_t *Tp = touched[nxt];
             for (int64_t k = t.rank(); k < ntouch_prev; k += t.size()) next_offer[Tp[k]] = 0ull;
-            for (int64_t k = t.rank(); k < ntouch; k += t.size()) {
-                const int32_t v = T0[k];
-                const unsigned long long o = cur_offer[v];
-                const int32_t b = (int32_t)(~(uint32_t)(o & 0xffffffffull));
-                const unsigned long long ob = cur_offer[b];
-                if (ob && (int32_t)(~(uint32_t)(ob & 0xffffffffull)) == v && v < b) {
-                    nm[b] = v;
-                    matched[v] = 1;
-                    matched[b] = 1;
-                    flags[it] = 1;
+            // (the pairs are counted at their smaller end, one atomic per warp)
+            int32_t mine = 0;
+            for (int64_t kb = t.rank() - lane_id(); kb < ntouch; kb += t.size()) {
+                const int64_t k = kb + lane_id();
+                if (k < ntouch) {
+                    const int32_t v = T0[k];
+                    const unsigned long long o = cur_offer[v];
+                    const int32_t b = (int32_t)(~(uint32_t)(o & 0xffffffffull));
+                    const unsigned long long ob = cur_offer[b];
+                    if (ob && (int32_t)(~(uint32_t)(ob & 0xffffffffull)) == v && v < b) {
+                        nm[b] = v;
+                        matched[v] = 1;
+                        matched[b] = 1;
+                        ++mine;
+                    }
                 }
             }
+            mine = warp_sum(mine);
+            if (lane_id() == 0 && mine) atomicAdd(&cnt_next[2], mine);
             t.sync();
             sc.alg_bytes += 12.0 * (double)nread + 24.0 * (double)ntouch;
-            // new pairs, each counted at its smaller end v: the only touched
-            // vertex that is matched and whose best offer b was mapped to it
-            const int32_t pairs = team_sum<Team, int32_t>(t, sc, sm, ntouch, [&](int64_t k) -> int32_t {
-                const int32_t v = T0[k];
-                const int32_t b = (int32_t)(~(uint32_t)(cur_offer[v] & 0xffffffffull));
-                return matched[v] && nm[b] == v ? 1 : 0;
-            });
+            const int32_t pairs = uread(&cnt_next[2]);
             const int32_t curm = prev + 2 * pairs;
             float rel = (float)(curm - prev) / ((float)prev + 1.0f);
             prev = curm;
             ntouch_prev = ntouch;
-            if (!uread(&flags[it]) || (double)rel < 0.1) break;
+            if (pairs == 0 || (double)rel < 0.1) break;
             // vertices matched in this iteration take no offers in the next:
             // the next offer pass reads `matched` after this sync
         }
         sc.arena.release(lm);
         prof_mark(t, sc, PH_MATCH_ITER);
     }
-    compress_labels(t, sc, sm, nm, M, M - 1, map_out);
+    // compress_label_sequence (include/rama_utils.h:160-177) of nm: the labels
+    // in use are exactly the roots (nm[v] == v; a matched vertex points to its
+    // smaller partner, which is a root), so a root's new label is its rank
+    // among the roots
+    int32_t *rank = reinterpret_cast<int32_t *>(offer[0]);  // the offers are dead by now
+    team_scan<Team, int64_t>(
+        t, sc, sm, M, [&](int64_t v) -> int64_t { return nm[v] == (int32_t)v ? 1 : 0; },
+        [&](int64_t v, int64_t pre, int64_t) { rank[v] = (int32_t)pre; });
+    for (int64_t v = t.rank(); v < M; v += t.size()) map_out[v] = rank[nm[v]];
+    t.sync();
     sc.arena.release(mark);
     return prev;
 }

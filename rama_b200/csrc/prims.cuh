@@ -78,7 +78,7 @@ enum Phase : int {
     PH_CONTRACT = 7,
     PH_OTHER = 8,
     PH_MATCH_ITER = 9,    // the offer / match iterations of a matching round
-    PH_CONTRACT_SORT = 10,  // the bucket sort of a contraction
+    PH_CSORT_BIG = 10,    // contraction sort: the buckets of more than BUCKET_MAX edges
     PH_CSR = 11,          // symmetric CSR builds (cycle search, forest)
     PH_CSORT_SLOT = 12,   // contraction sort: endpoints and bucket slots
     PH_CSORT_SCATTER = 13,  // ... bucket starts and the scatter
@@ -327,17 +327,22 @@ __device__ void team_maxi_minf(const Team &t, Scratch &sc, char *sm, int64_t n, 
 // ---------------------------------------------------------------------------
 // team exclusive scan: out(i, prefix, value) is called for every i in [0,n)
 // in chunk order; returns the total.  Two team syncs; outputs are visible to
-// the whole team on return.  The second pass takes tiles of SCAN_ITEMS
-// consecutive elements per thread: a serial scan in registers and one block
-// scan per tile (one block scan per SCAN_ITEMS x blockDim elements keeps the
-// CTA's barriers few).  Integer sums only, so the result does not depend on
-// the tiling.
+// the whole team on return.  The second pass takes tiles of blockDim * ITEMS
+// elements (ITEMS = 4 for 8-byte sums, 8 for 4-byte ones): each warp a contiguous segment of 32 * SCAN_ITEMS,
+// lane l its elements l, l + 32, ... (coalesced loads); the warp scans them
+// in order with shuffles, and one block scan of the warp totals per tile
+// keeps the CTA's barriers few.  Integer sums only, so the result does not
+// depend on the tiling.
 // ---------------------------------------------------------------------------
-constexpr int SCAN_ITEMS = 8;
+template <class T>
+struct ScanItems {
+    static constexpr int value = sizeof(T) == 8 ? 4 : 8;
+};
 
 template <class Team, class T, class In, class Out>
 __device__ T team_scan(const Team &t, Scratch &sc, char *sm, int64_t n, In in, Out out)
 {
+    constexpr int ITEMS = ScanItems<T>::value;
     T *tsm = reinterpret_cast<T *>(sm);
     int64_t lo, hi;
     block_chunk(t, n, lo, hi);
@@ -355,23 +360,26 @@ __device__ T team_scan(const Team &t, Scratch &sc, char *sm, int64_t n, In in, O
     }
     base = warp_sum(base);
     total = warp_sum(total);
-    const int64_t TILE = (int64_t)blockDim.x * SCAN_ITEMS;
+    const int64_t TILE = (int64_t)blockDim.x * ITEMS;
+    const int64_t wseg = (int64_t)warp_in_block() * 32 * ITEMS;
     for (int64_t tile = lo; tile < hi; tile += TILE) {
-        const int64_t i0 = tile + (int64_t)threadIdx.x * SCAN_ITEMS;
-        T v[SCAN_ITEMS];
-        T mine = T(0);
+        const int64_t i0 = tile + wseg + lane_id();
+        T v[ITEMS], ex[ITEMS];
 #pragma unroll
-        for (int k = 0; k < SCAN_ITEMS; ++k) {
-            v[k] = i0 + k < hi ? in(i0 + k) : T(0);
-            mine += v[k];
+        for (int k = 0; k < ITEMS; ++k) v[k] = i0 + 32 * k < hi ? in(i0 + 32 * k) : T(0);
+        T wrun = T(0);
+#pragma unroll
+        for (int k = 0; k < ITEMS; ++k) {
+            const T x = warp_incl_scan(v[k]);
+            ex[k] = wrun + x - v[k];
+            wrun += __shfl_sync(FULL, x, 31);
         }
         T ts;
-        T run = base + block_excl_scan<T>(mine, tsm, ts);
+        const T wofs = base + block_excl_scan<T>(lane_id() == 0 ? wrun : T(0), tsm, ts);
+        const T wbase = __shfl_sync(FULL, wofs, 0);
 #pragma unroll
-        for (int k = 0; k < SCAN_ITEMS; ++k) {
-            if (i0 + k < hi) out(i0 + k, run, v[k]);
-            run += v[k];
-        }
+        for (int k = 0; k < ITEMS; ++k)
+            if (i0 + 32 * k < hi) out(i0 + 32 * k, wbase + ex[k], v[k]);
         base += ts;
     }
     t.sync();
@@ -421,41 +429,67 @@ __device__ __forceinline__ csum_t cs_warp_tree(csum_t a)
     return a;
 }
 
-// returns the sum on every thread; two team syncs
-template <class Team, class Get>
-__device__ double team_csum(const Team &t, Scratch &sc, int64_t n, Get get)
+// returns the sum on every thread; two team syncs.  *count receives the
+// number of k with cnt(k) (an exact integer sum computed in the same pass).
+template <class Team, class Get, class Cnt>
+__device__ double team_csum_count(const Team &t, Scratch &sc, int64_t n, Get get, Cnt cnt, int64_t *count)
 {
     const int64_t nch = (n + 4095) / 4096;
     uint64_t m = sc.arena.mark();
     csum_t *parts = sc.arena.take<csum_t>(nch + 1);
+    int64_t *pcnt = sc.arena.take<int64_t>(nch + 1);
     double *res = reinterpret_cast<double *>(sc.next_part());
     if (sc.arena.ok()) {
         const int64_t w = team_warp(t), nw = team_nwarps(t);
         for (int64_t ch = w; ch < nch; ch += nw) {
             csum_t a = {0.0, 0.0};
+            int64_t c = 0;
             const int64_t b0 = ch * 4096 + lane_id();
             for (int k = 0; k < 128; ++k) {
                 int64_t idx = b0 + 32 * k;
-                if (idx < n) a = cs_merge(a, csum_t{get(idx), 0.0});
+                if (idx < n) {
+                    a = cs_merge(a, csum_t{get(idx), 0.0});
+                    c += cnt(idx) ? 1 : 0;
+                }
             }
             a = cs_warp_tree(a);
-            if (lane_id() == 0) parts[ch] = a;
+            c = warp_sum(c);
+            if (lane_id() == 0) {
+                parts[ch] = a;
+                pcnt[ch] = c;
+            }
         }
     }
     t.sync();
     if (sc.arena.ok() && t.block() == 0 && warp_in_block() == 0) {
         csum_t a = {0.0, 0.0};
-        for (int64_t k = lane_id(); k < nch; k += 32) a = cs_merge(a, parts[k]);
+        int64_t c = 0;
+        for (int64_t k = lane_id(); k < nch; k += 32) {
+            a = cs_merge(a, parts[k]);
+            c += pcnt[k];
+        }
         a = cs_warp_tree(a);
-        if (lane_id() == 0) res[0] = __dadd_rn(a.s, a.c);
+        c = warp_sum(c);
+        if (lane_id() == 0) {
+            res[0] = __dadd_rn(a.s, a.c);
+            reinterpret_cast<int64_t *>(res)[1] = c;
+        }
     }
     t.sync();
     double r = uread(&res[0]);
+    *count = uread(&reinterpret_cast<int64_t *>(res)[1]);
     sc.arena.release(m);
     // `res` lies in one of the two partial buffers: the next primitive uses the
     // other one, and the one after it can write this one only after a team
     // sync that every thread reaches after this read
     return r;
+}
+
+template <class Team, class Get>
+__device__ double team_csum(const Team &t, Scratch &sc, int64_t n, Get get)
+{
+    int64_t unused = 0;
+    return team_csum_count(t, sc, n, get, [](int64_t) { return false; }, &unused);
 }
 
 // RSUM over values v(k), k in [0,n) by ONE thread (n <= 32): the oracle's
@@ -1015,6 +1049,7 @@ __device__ bool team_bucket_sort_ex(const Team &t, Scratch &sc, char *sm, int64_
         }
     }
     t.sync();
+    if (detail_phase >= 0) prof_mark(t, sc, detail_phase + 2);
     // (compiled only for callers that give a big key)
     if constexpr (!std::is_same<BigKey, NoBigKey>::value) if (has_big) {
         // the buckets beyond BUCKET_MAX: their items in input order, a stable
@@ -1053,8 +1088,8 @@ __device__ bool team_bucket_sort_ex(const Team &t, Scratch &sc, char *sm, int64_
         }
         t.sync();
         sc.arena.release(bm);
+        if (detail_phase >= 0) prof_mark(t, sc, PH_CSORT_BIG);
     }
-    if (detail_phase >= 0) prof_mark(t, sc, detail_phase + 2);
     sc.arena.release(am);
     return true;
 }
