@@ -42,6 +42,8 @@ CONFIGS = {
     "c3": dict(desc="random geometric k-NN graph, 1M points, k=20, D (dual only)", mode="D"),
     "c4": dict(desc="512 Delaunay region-adjacency graphs, n log-uniform [500,20000], batched PD", mode="PD"),
     "c2s": dict(desc="3-D grid 64x64x32 + long range (profiling-size C2), PD", mode="PD"),
+    "c4s": dict(desc="64 Delaunay region-adjacency graphs of the C4 generator (profiling size), batched PD",
+                mode="PD"),
     "c5": dict(desc="served: Poisson arrivals of grids 16^3..128^3, Delaunay 1e3..2e6 edges, k-NN (k=10) "
                     "1e4..5e5 nodes; modes P/PD/D 50/40/10%", mode="mixed"),
 }
@@ -200,7 +202,7 @@ def run_ours(args, rank, world, local):
     torch.cuda.set_device(local)
     cfg = args.config
     mode = CONFIGS[cfg]["mode"]
-    if cfg == "c4":
+    if cfg in ("c4", "c4s"):
         return run_ours_batch(args, rank, world, local)
     if cfg == "c5":
         return run_ours_served(args, rank, world, local)
@@ -352,7 +354,7 @@ def run_ours_batch(args, rank, world, local):
     from rama_b200 import instances as I
     from rama_b200.solver import Solver
 
-    batch = I.delaunay_batch(seed=1004 + rank)
+    batch = I.delaunay_batch(count=64 if args.config == "c4s" else 512, seed=1004 + rank)
     dev = torch.device("cuda", local)
     d_i = torch.from_numpy(batch.i).to(dev)
     d_j = torch.from_numpy(batch.j).to(dev)
@@ -405,7 +407,7 @@ def run_ours_batch(args, rank, world, local):
         "metric": "edges/s", "value": value, "unit": "edges/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32 (costs, messages) / f64 (bound, objective)", "data": "synthetic",
-        "config": {"workload": CONFIGS["c4"]["desc"], "instances": batch.count, "edges": E,
+        "config": {"workload": CONFIGS[args.config]["desc"], "instances": batch.count, "edges": E,
                    "parallelism": "instances dealt to CTAs, largest first; ranks hold separate batches"},
         "solves_per_s": world * batch.count * args.steps / (ms / 1e3),
         "plain": {"value": E / (plain_ms / 1e3), "unit": "edges/s", "device_ms": plain_ms, "wall_s": plain_wall,
@@ -442,7 +444,10 @@ def run_ours_served(args, rank, world, local):
     pinned = [tuple(torch.from_numpy(np.ascontiguousarray(x)).pin_memory() for x in g) for g in pool]
     nodes = [int(max(g[0].max(), g[1].max())) + 1 for g in pool]
     gen_s = time.perf_counter() - t_gen
-    srv = S.Server(device=local, lanes=args.lanes, lane_bytes=args.lane_gb << 30, max_batch=256)
+    tsolver = Solver(local)
+    tuning = tune_solver(tsolver, local, args)
+    srv = S.Server(device=local, lanes=args.lanes, lane_bytes=args.lane_gb << 30, max_batch=256,
+                   tuning=tsolver.handle.tuning())
     # warm-up: every pool graph once, all queued at once
     warm = [S.Request(k, *pinned[k], mode="PD", num_nodes=nodes[k]) for k in range(len(pool))]
     for _ in range(max(1, args.warmup // 3)):
@@ -487,9 +492,10 @@ def run_ours_served(args, rank, world, local):
         "data": "synthetic (seeded pool of request graphs with the served mix's kinds and size ranges)",
         "config": {"workload": CONFIGS["c5"]["desc"], "requests_per_rate": args.requests, "rates_per_s": rates,
                    "pool_graphs": len(pool), "pool_edges": int(sum(len(g[2]) for g in pool)),
-                   "lanes": args.lanes, "lane_bytes": args.lane_gb << 30,
-                   "parallelism": "continuous batching: lanes = handle + stream + fixed HBM budget; instances "
-                                  "on 8-CTA clusters or one CTA each"},
+                   "lanes": args.lanes, "lane_bytes": args.lane_gb << 30, "solo_min_edges": srv.solo_min_edges,
+                   "parallelism": "continuous batching: lanes = handle + stream + fixed HBM budget; requests of "
+                                  "solo_min_edges or more alone on the whole GPU, the rest batched on clusters "
+                                  "or one CTA each"},
         "solves_per_s": world * top["solves_per_s"],
         "served": per_rate,
         "plain": {"value": plain_edges / (plain_ms / 1e3) if plain_ms else 0.0, "unit": "edges/s",
@@ -503,6 +509,7 @@ def run_ours_served(args, rank, world, local):
                      "algorithmic_bytes": alg, "note": "algorithmic bytes of all served batches / served wall time"},
         "pool_generation_s": gen_s,
         "clocks": clk.summary(),
+        "tuning": tuning,
     }
 
 

@@ -141,6 +141,8 @@ int rama_solve_batch(rama_handle h, const int32_t *d_i, const int32_t *d_j, cons
  * then fills the host result arrays.  opts holds 1 entry (shared) or `count`
  * entries (per instance).  Each instance gets a workspace slice sized from
  * its edge count (about 1 KiB per edge); the sum is the batch's footprint.
+ * A batch of one instance whose options ask for team 2 runs on the whole GPU
+ * (a cooperative launch; it starts once the SMs are free of other kernels).
  * One batch in flight per handle: a server keeps one handle per concurrent
  * batch.  No counterpart in the reference (it solves one instance per call).
  */

@@ -677,7 +677,12 @@ int rama_batch_launch(rama_handle h, const int32_t *d_i, const int32_t *d_j, con
     CU(cudaMemcpyAsync(h->d_inst, h->b_host, sizeof(Instance) * count, cudaMemcpyHostToDevice, st));
     CU(cudaMemcpyAsync(h->d_order, h->b_order.data(), sizeof(int32_t) * count, cudaMemcpyHostToDevice, st));
     CU(cudaEventRecord(h->ev0, st));
-    rc = launch_solve(h, count, 1, st, ncluster);
+    // a batch of one instance that asks for the whole GPU (team 2) runs on
+    // the cooperative grid, in its slice at the start of the workspace
+    if (count == 1 && opts[0].team == 2)
+        rc = launch_solve(h, 1, 2, st, 0, h->b_in[0].n);
+    else
+        rc = launch_solve(h, count, 1, st, ncluster);
     if (rc) return rc;
     CU(cudaEventRecord(h->ev1, st));
     CU(cudaMemcpyAsync(h->b_host, h->d_inst, sizeof(Instance) * count, cudaMemcpyDeviceToHost, st));

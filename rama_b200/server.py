@@ -11,8 +11,11 @@ footprint is its workspace slice, 1024 bytes per edge plus 1 MiB, as the
 solver allocates it, plus 16 bytes per edge and 4 per node of inputs and
 labels).  It copies their graphs to the device and launches them as one
 asynchronous batch (``rama_batch_launch``: instances that hold much more
-than the batch's load per CTA run on 8-CTA cluster teams, the rest one per
-CTA).
+than the batch's load per CTA run on cluster teams, the rest one per CTA).
+A request of at least `solo_min_edges` edges (default: the size from which a
+single solve runs on the whole GPU, from the handle's tuning) is launched
+alone, on the whole GPU: on one CTA or one cluster it would take many times
+longer than a plain solve, and every request queued behind it would wait.
 
 Lanes run concurrently on their own streams, so the kernels of requests
 admitted at different times overlap on the GPU.  A lane that finishes hands
@@ -141,7 +144,7 @@ class Lane:
     def handle_ws(self) -> int:
         return max(self.budget - 16 * self.io_edges - 4 * self.io_nodes, 64 * MiB)
 
-    def launch(self, group: List[Request], now: float):
+    def launch(self, group: List[Request], now: float, solo: bool = False):
         import torch
 
         n = len(group)
@@ -156,7 +159,7 @@ class Lane:
                     self.d_i[a:b].copy_(_as_tensor(r.i), non_blocking=True)
                     self.d_j[a:b].copy_(_as_tensor(r.j), non_blocking=True)
                     self.d_c[a:b].copy_(_as_tensor(r.c), non_blocking=True)
-        opts = (_lib.RamaOptions * n)(*[_lib.options(r.mode) for r in group])
+        opts = (_lib.RamaOptions * n)(*[_lib.options(r.mode, team=2 if solo else 0) for r in group])
         st = C.c_void_p(self.stream.cuda_stream)
         _lib.check(_lib.load().rama_batch_launch(self.handle.h, self.d_i.data_ptr(), self.d_j.data_ptr(),
                                                  self.d_c.data_ptr(), eo.ctypes.data, n, opts, n,
@@ -235,14 +238,21 @@ class Server:
     """Continuous batching over `lanes` lanes of `lane_bytes` of HBM each."""
 
     def __init__(self, device: int = 0, lanes: int = 8, lane_bytes: int = 8 << 30, max_batch: int = 256,
-                 io_edges: Optional[int] = None, io_nodes: Optional[int] = None):
+                 io_edges: Optional[int] = None, io_nodes: Optional[int] = None,
+                 solo_min_edges: Optional[int] = None, tuning=None):
         if io_edges is None:
             io_edges = lane_bytes // 1100
         if io_nodes is None:
             io_nodes = io_edges
         self.max_batch = max_batch
         self.lanes = [Lane(k, device, lane_bytes, io_edges, io_nodes) for k in range(lanes)]
+        if tuning is not None:
+            for ln in self.lanes:
+                ln.handle.set_tuning(tuning)
         self.lane_bytes = lane_bytes
+        if solo_min_edges is None:
+            solo_min_edges = int(self.lanes[0].handle.tuning().single_grid_min)
+        self.solo_min_edges = solo_min_edges
 
     def close(self):
         for ln in self.lanes:
@@ -251,12 +261,24 @@ class Server:
     def admissible(self, r: Request) -> bool:
         return self.lanes[0].fits([r])
 
-    def _take(self, pending: deque, lane: Lane) -> List[Request]:
+    def _take(self, pending: deque, lane: Lane):
+        """The next group for `lane` and whether it runs alone on the whole
+        GPU: a large request at the front of the queue goes alone; otherwise
+        the small requests up to the next large one, by footprint."""
+        if pending and pending[0].num_edges >= self.solo_min_edges:
+            return [pending.popleft()], True
         group = admit(pending, lane.budget, self.max_batch)
+        # a large request ends the group (it runs alone later)
+        for k, r in enumerate(group):
+            if r.num_edges >= self.solo_min_edges:
+                for x in reversed(group[k:]):
+                    pending.appendleft(x)
+                group = group[:k]
+                break
         # the I/O buffers and the workspace bound the group too
         while group and not lane.fits(group):
             pending.appendleft(group.pop())
-        return group
+        return group, False
 
     def serve(self, requests: Sequence[Request], clock: Callable[[], float] = time.perf_counter,
               realtime: bool = True) -> ServeStats:
@@ -292,9 +314,9 @@ class Server:
                     progressed = True
             for ln in self.lanes:
                 if not ln.busy and pending:
-                    group = self._take(pending, ln)
+                    group, solo = self._take(pending, ln)
                     if group:
-                        ln.launch(group, clock() - t0)
+                        ln.launch(group, clock() - t0, solo=solo)
                         stats.batches += 1
                         progressed = True
             stats.max_busy_lanes = max(stats.max_busy_lanes, sum(ln.busy for ln in self.lanes))

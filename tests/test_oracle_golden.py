@@ -261,23 +261,45 @@ def test_fixture_full_solve_primal(oracle, F, k):
     assert _valid_multicut(i, j, lab)
 
 
-@pytest.mark.parametrize("k", CASES)
-@pytest.mark.parametrize("mode", ("PD", "PD+"))
-def test_fixture_full_solve_dual_modes(oracle, F, k, mode):
-    """With the default triangle budget the reference truncates its triangle
-    set nondeterministically on these instances; the oracle's solution must be
-    a partition of all nodes with LB <= objective, and its objective close to
-    the reference's (untruncated runs are compared tightly in
-    test_untruncated_full_solves).  Clusters need not be connected in the
-    input graph: the dual adds triangle chords that later rounds contract,
-    in the reference as well."""
-    i, j, c = (_g(F, f"init{k}", x) for x in "ijc")
-    lab, lb, _ = oracle.solve(i, j, c, mode)
-    assert len(lab) == int(max(i.max(), j.max())) + 1 and lab.min() >= 0
-    obj = oracle.objective(i, j, c, lab)
-    assert lb <= obj + 1e-6
-    ref_obj = oracle.objective(i, j, c, _g(F, f"rama{k}_{mode}", "labels"))
-    assert abs(obj - ref_obj) <= 0.1 * max(1.0, abs(ref_obj))
+def _recorded_spread(F):
+    """The reference's run-to-run spread of the PD objective on the spread
+    graphs (5 runs each, default budget): (max - min) / |mean|, largest."""
+    keys = sorted({k.split("/")[0] for k in F.files if k.startswith("spread")})
+    worst = 0.0
+    for name in keys:
+        o = _g(F, name, "obj")
+        worst = max(worst, float((o.max() - o.min()) / max(1.0, abs(o.mean()))))
+    return worst
+
+
+def test_fixture_full_solves_dual_modes(oracle, F):
+    """PD and PD+ with the default triangle budget, every fixture graph.  Where
+    no cycle search truncated, the oracle's objective equals the reference's.
+    Where the budget truncates, the reference keeps whichever triangles its
+    atomics admit and its own objective varies from run to run (up to the
+    recorded spread, 15.6 % on these graphs); the oracle's objective must lie
+    within that spread of the reference's, and must not be worse on average
+    (mean signed gap at most 0.5 %).  Every solution is a partition of all
+    nodes with LB <= objective.  Clusters need not be connected in the input
+    graph: the dual adds triangle chords that later rounds contract, in the
+    reference as well."""
+    spread = _recorded_spread(F)
+    assert spread > 0.0
+    gaps = []
+    for k in CASES:
+        i, j, c = (_g(F, f"init{k}", x) for x in "ijc")
+        for mode in ("PD", "PD+"):
+            lab, lb, st = oracle.solve(i, j, c, mode)
+            assert len(lab) == int(max(i.max(), j.max())) + 1 and lab.min() >= 0
+            obj = oracle.objective(i, j, c, lab)
+            assert lb <= obj + 1e-6
+            ref_obj = oracle.objective(i, j, c, _g(F, f"rama{k}_{mode}", "labels"))
+            gap = (obj - ref_obj) / max(1.0, abs(ref_obj))  # > 0: worse than the reference
+            if st.truncations == 0:
+                assert abs(gap) <= 1e-6, (k, mode, obj, ref_obj)
+            assert abs(gap) <= spread, (k, mode, gap, spread)
+            gaps.append(gap)
+    assert float(np.mean(gaps)) <= 5e-3, gaps
 
 
 def test_untruncated_full_solves(oracle, F):
@@ -306,17 +328,28 @@ def test_untruncated_full_solves(oracle, F):
     assert compared > 0
 
 
-def test_reference_spread(F):
-    """Records how far the reference disagrees with itself (5 runs, default
-    budget): the tolerance any full-solve comparison with it can expect."""
+def test_reference_spread(oracle, F):
+    """The reference disagrees with itself once its triangle budget truncates
+    (5 runs, default budget): its objective and bound move from run to run on
+    these graphs.  The oracle's bound on each of them lies inside the
+    reference's range of bounds, widened by the largest spread of the bound
+    seen on any of them."""
     keys = sorted({k.split("/")[0] for k in F.files if k.startswith("spread")})
     if not keys:
         pytest.skip("fixture file predates the spread cases")
-    worst = 0.0
+    assert _recorded_spread(F) > 1e-3
+    lb_spread = 0.0
     for name in keys:
         lb = _g(F, name, "lb")
-        worst = max(worst, (lb.max() - lb.min()) / max(1.0, abs(lb.mean())))
-    assert worst >= 0.0
+        lb_spread = max(lb_spread, float((lb.max() - lb.min()) / max(1.0, abs(lb.mean()))))
+    assert lb_spread > 1e-4
+    for name in keys:
+        k = int(name[len("spread"):])
+        i, j, c = (_g(F, f"init{k}", x) for x in "ijc")
+        _, lb, _ = oracle.solve(i, j, c, "PD")
+        ref = _g(F, name, "lb")
+        scale = max(1.0, abs(ref.mean()))
+        assert ref.min() - lb_spread * scale <= lb <= ref.max() + lb_spread * scale, (name, lb, ref)
 
 
 @pytest.mark.parametrize("k", range(4))

@@ -28,6 +28,24 @@ def test_admit_never_skips_the_front_request():
     assert [r.rid for r in q] == [0, 1]
 
 
+def _sreq(edges, rid):
+    return SimpleNamespace(bytes=edges * 1100, num_edges=edges, num_nodes=edges, rid=rid)
+
+
+def test_large_requests_go_alone_and_end_a_group():
+    """A request of at least solo_min_edges runs alone (on the whole GPU); a
+    group of small ones stops in front of it, and it is taken next."""
+    me = SimpleNamespace(solo_min_edges=1000, max_batch=10)
+    lane = SimpleNamespace(budget=10 ** 9, fits=lambda g: True)
+    q = deque([_sreq(10, 0), _sreq(20, 1), _sreq(5000, 2), _sreq(30, 3)])
+    g, solo = server.Server._take(me, q, lane)
+    assert [r.rid for r in g] == [0, 1] and not solo
+    g, solo = server.Server._take(me, q, lane)
+    assert [r.rid for r in g] == [2] and solo
+    g, solo = server.Server._take(me, q, lane)
+    assert [r.rid for r in g] == [3] and not solo and not q
+
+
 def test_footprint_counts_the_solver_slice():
     # the solver's slice: 1024 B per edge + 1 MiB, rounded up to 4 KiB
     assert server.workspace_slice(0) == 1 << 20
@@ -53,7 +71,8 @@ def test_results_in_the_mix_equal_solo_solves():
 
     pool = instances.served_pool(size=10, seed=21, max_edges=60000)
     stream = instances.served_stream(num_requests=30, rate=3000.0, pool_size=10, seed=22)
-    srv = server.Server(device=0, lanes=3, lane_bytes=512 << 20, max_batch=8)
+    # requests of 20,000 edges and more run alone on the whole GPU
+    srv = server.Server(device=0, lanes=3, lane_bytes=512 << 20, max_batch=8, solo_min_edges=20000)
     try:
         reqs = [server.Request(k, *pool[p], mode=m, arrival=t) for k, (t, m, p) in enumerate(stream)]
         st = srv.serve(reqs, realtime=True)
