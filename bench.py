@@ -58,17 +58,23 @@ def peaks():
     return 6650.0, "fallback"
 
 
-# DRAM traffic of one k_solve_grid launch (dram__bytes_read.sum +
-# dram__bytes_write.sum), per input edge, from one ncu capture of the
-# profiling-size C2 case (3-D grid 64x64x32 + long range, 753,664 edges, PD):
-# 344,752,640 B read + 1,458,030,592 B written.  The full C2 instance is too
-# large to capture under replay; algorithmic bytes per edge are the same for
-# both sizes (1097 vs 1096 B/edge), so the traffic is scaled by edge count.
-# Command: ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
+# DRAM traffic (dram__bytes_read.sum + dram__bytes_write.sum) of one solve
+# launch per input edge, from one ncu capture of a profiling-size case of the
+# same generator; the full instances are too large to capture under replay,
+# so the traffic is scaled by edge count (the algorithmic bytes per edge of
+# the two sizes are close: see roofline.algorithmic_bytes).
+#   C2 (k_solve_grid), 3-D grid 64x64x32 + long range, 753,664 edges, PD:
+#     193,286,912 B read + 990,223,872 B written;
+#   C4 (k_solve_mixed), 64 Delaunay graphs of the C4 generator, 1,048,829
+#     edges, PD: 369,878,784 B read + 1,887,969,536 B written.
+# Commands: ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
 #   --clock-control none -k regex:k_solve_grid -s 1 -c 1
-#   python bench.py --config c2s --steps 2 --warmup 1 --no-cpu-baseline
-TRAFFIC_B_PER_EDGE = {("c2", "PD"): (344752640 + 1458030592) / 753664,
-                      ("c2s", "PD"): (344752640 + 1458030592) / 753664}
+#   python bench.py --config c2s --steps 2 --warmup 1 --no-cpu-baseline --no-tune
+# (and -k regex:k_solve_ -s 1 -c 2 ... --config c4s --steps 3 --warmup 3 for C4)
+TRAFFIC_B_PER_EDGE = {("c2", "PD"): (193286912 + 990223872) / 753664,
+                      ("c2s", "PD"): (193286912 + 990223872) / 753664,
+                      ("c4", "PD"): (369878784 + 1887969536) / 1048829,
+                      ("c4s", "PD"): (369878784 + 1887969536) / 1048829}
 
 
 def make_instance(cfg):
@@ -403,6 +409,7 @@ def run_ours_batch(args, rank, world, local):
     hbm, src = peaks()
     achieved = float(stats.alg_bytes) / (stats.device_ms / 1e3) / 1e9 if stats.device_ms else 0.0
     value = world * E * args.steps / (ms / 1e3)
+    tpe = TRAFFIC_B_PER_EDGE.get((args.config, "PD"))
     return {
         "metric": "edges/s", "value": value, "unit": "edges/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -414,7 +421,8 @@ def run_ours_batch(args, rank, world, local):
                   "form": "one instance per launch"},
         "gpu_launches": args.steps,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s", "frac": achieved / hbm,
-                     "traffic": None, "peak_source": src, "kernel": "k_solve_cta", "kernel_ms": stats.device_ms,
+                     "traffic": tpe * E if tpe else None, "peak_source": src,
+                     "kernel": "k_solve_mixed / k_solve_cta", "kernel_ms": stats.device_ms,
                      "algorithmic_bytes": float(stats.alg_bytes)},
         "clocks": clk.summary(),
         "tuning": tuning,

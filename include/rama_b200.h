@@ -217,6 +217,8 @@ typedef struct {
     int64_t batch_cluster_min;   /* batch instances below this size always run on one CTA; larger ones on */
     float batch_cluster_share;   /* a cluster when they hold more than this many times the batch's edges
                                     per CTA */
+    int32_t cta_threads;         /* threads of a CTA that solves instances alone: 512 (two per SM) or
+                                    256 (three per SM, more instances in flight) */
 } rama_tuning;
 int rama_get_tuning(rama_handle h, rama_tuning *out);
 /* RAMA_ERR_INVALID_ARG for a value outside its range or a cluster size that

@@ -70,6 +70,7 @@ class RamaTuning(C.Structure):
         ("single_grid_min", C.c_int64),
         ("batch_cluster_min", C.c_int64),
         ("batch_cluster_share", C.c_float),
+        ("cta_threads", C.c_int32),
     ]
 
     def as_dict(self):

@@ -16,8 +16,10 @@ built-in choices are guesses; this module measures them on the device:
   CTA to a cluster and from a cluster to the whole GPU -- each team is timed
   on graphs of increasing size and the switch goes to the first size at which
   the larger team wins;
-* batch_cluster_min / batch_cluster_share: which instances of a batch get a
-  cluster, timed on a batch of Delaunay graphs of uneven size.
+* batch_cluster_min / batch_cluster_share / cta_threads: which instances of
+  a batch get a cluster, and whether the instances solved alone take CTAs of
+  512 threads (two per SM) or 256 (three per SM), timed together on a batch
+  of Delaunay graphs of uneven size.
 
 Every trial solve's labels and bound are checked to equal the first trial's:
 a tuning never changes a result, and the tuner fails loudly if one would.
@@ -42,7 +44,7 @@ from . import _lib
 from . import instances as I
 
 KNOBS = ("grid_ctas_per_sm", "grid_small_ctas_per_sm", "grid_small_max", "cluster_ctas", "single_cluster_min",
-         "single_grid_min", "batch_cluster_min", "batch_cluster_share")
+         "single_grid_min", "batch_cluster_min", "batch_cluster_share", "cta_threads")
 
 
 def cache_path() -> str:
@@ -240,15 +242,18 @@ def tune(device: int = 0, budget_s: float = 60.0, quick: bool = False) -> dict:
 
     # batches: which instances get a cluster
     batch = I.delaunay_batch(count=96 if not quick else 24, nmin=500, nmax=20000, seed=11)
+    # (and the CTA size of the instances that run alone: a batch without
+    # cluster instances runs on the per-instance CTA kernel of that size)
     tb = {}
-    for bmin, share in ((10000, 1.0), (20000, 1.5), (20000, 3.0), (40000, 1.5), (1 << 40, 1.5)):
-        if time.perf_counter() - t0 > budget_s and tb:
-            break
-        tr.set(**{**chosen, "batch_cluster_min": bmin, "batch_cluster_share": share})
-        tb[(bmin, share)] = tr.batch("batch", batch, "PD")
-    bmin, share = pick_fastest(tb)
-    chosen["batch_cluster_min"], chosen["batch_cluster_share"] = bmin, share
-    tables["batch"] = {f"{k[0]}/{k[1]}": v for k, v in tb.items()}
+    for threads in (512, 256):
+        for bmin, share in ((10000, 1.0), (20000, 1.5), (20000, 3.0), (40000, 1.5), (1 << 40, 1.5)):
+            if time.perf_counter() - t0 > budget_s and tb:
+                break
+            tr.set(**{**chosen, "batch_cluster_min": bmin, "batch_cluster_share": share, "cta_threads": threads})
+            tb[(bmin, share, threads)] = tr.batch("batch", batch, "PD")
+    bmin, share, threads = pick_fastest(tb)
+    chosen["batch_cluster_min"], chosen["batch_cluster_share"], chosen["cta_threads"] = bmin, share, threads
+    tables["batch"] = {f"{k[0]}/{k[1]}/{k[2]}": v for k, v in tb.items()}
     tr.set(**chosen)
     return {"tuning": chosen, "default": base, "tables": tables, "seconds": round(time.perf_counter() - t0, 1)}
 

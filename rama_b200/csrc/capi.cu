@@ -91,6 +91,7 @@ struct rama_context {
     int step_ctas = 0;  // ... of k_step_grid
     int obj_ctas = 0;   // ... of k_objective
     int cta_per_sm = 0;
+    int cta_small_per_sm = 0;  // co-resident CTAs of k_solve_cta_small per SM
     int grid_per_sm_max = 0;  // occupancy maximum of k_solve_grid per SM
     int cluster_cap[17] = {};  // co-resident clusters of k_solve_mixed by cluster size (0: not known yet)
     rama_tuning tune{};
@@ -255,10 +256,15 @@ int launch_solve(rama_context *h, int32_t count, int team, cudaStream_t st, int3
         cfg.numAttrs = 1;
         CU(cudaLaunchKernelEx(&cfg, k_solve_mixed, L));
     } else {
-        const int ctas = std::max(1, std::min<int>(count, h->sms * h->cta_per_sm));
         CU(cudaMemsetAsync(h->d_queue, 0, sizeof(int32_t), st));
         CtaLaunch L{h->d_inst, h->d_order, count, h->d_queue};
-        k_solve_cta<<<ctas, THREADS, SMEM, st>>>(L);
+        if (h->tune.cta_threads == THREADS_SMALL) {
+            const int ctas = std::max(1, std::min<int>(count, h->sms * h->cta_small_per_sm));
+            k_solve_cta_small<<<ctas, THREADS_SMALL, SMEM_SMALL, st>>>(L);
+        } else {
+            const int ctas = std::max(1, std::min<int>(count, h->sms * h->cta_per_sm));
+            k_solve_cta<<<ctas, THREADS, SMEM, st>>>(L);
+        }
         CU(cudaGetLastError());
     }
     return RAMA_OK;
@@ -456,6 +462,7 @@ int rama_create(int device, uint64_t workspace_bytes, rama_handle *out)
     h->tune.single_grid_min = DEFAULT_SINGLE_GRID_MIN;
     h->tune.batch_cluster_min = DEFAULT_BATCH_CLUSTER_MIN;
     h->tune.batch_cluster_share = DEFAULT_BATCH_CLUSTER_SHARE;
+    h->tune.cta_threads = THREADS;
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_step_grid, THREADS, SMEM));
     h->step_ctas = std::max(1, per_sm) * h->sms;
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_objective, THREADS, SMEM));
@@ -465,6 +472,10 @@ int rama_create(int device, uint64_t workspace_bytes, rama_handle *out)
     int per_sm_cta = 0;
     CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_cta, k_solve_cta, THREADS, SMEM));
     h->cta_per_sm = std::max(1, per_sm_cta);
+    CU(cudaFuncSetAttribute((const void *)k_solve_cta_small, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                            SMEM_SMALL));
+    CU(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_cta, k_solve_cta_small, THREADS_SMALL, SMEM_SMALL));
+    h->cta_small_per_sm = std::max(1, per_sm_cta);
     if (cluster_capacity(h, DEFAULT_CLUSTER_CTAS) < 1) {
         delete h;
         return fail(RAMA_ERR_CUDA, "no cluster of the solver kernel fits on the device");
@@ -802,6 +813,9 @@ int rama_set_tuning(rama_handle h, const rama_tuning *t)
     if (!(c == 2 || c == 4 || c == 8 || c == 16)) return fail(RAMA_ERR_INVALID_ARG, "cluster_ctas must be 2, 4, 8 or 16");
     if (cluster_capacity(h, c) < 1)
         return fail(RAMA_ERR_INVALID_ARG, "no cluster of " + std::to_string(c) + " CTAs fits on this device");
+    if (t->cta_threads != THREADS && t->cta_threads != THREADS_SMALL)
+        return fail(RAMA_ERR_INVALID_ARG, "cta_threads must be " + std::to_string(THREADS) + " or " +
+                                              std::to_string(THREADS_SMALL));
     if (t->single_cluster_min < 0 || t->single_grid_min < 0 || t->batch_cluster_min < 0 ||
         !(t->batch_cluster_share > 0.0f))
         return fail(RAMA_ERR_INVALID_ARG, "thresholds must be non-negative and the share positive");

@@ -11,6 +11,16 @@ namespace rama {
 
 constexpr int THREADS = 512;
 constexpr int SMEM = sort_smem_bytes(THREADS) + 1024;
+static_assert(THREADS / 32 * 1024 + BUCKET_MAX * 12 <= sort_smem_bytes(THREADS),
+              "the CTA bucket sort's staging area fits");
+// the smaller CTA of k_solve_cta_small (the autotuner chooses between the two
+// for CTA-team solves); its shared memory also holds a CTA bucket sort of
+// BUCKET_MAX items
+constexpr int THREADS_SMALL = 256;
+constexpr int SMEM_SMALL = (sort_smem_bytes(THREADS_SMALL) > THREADS_SMALL / 32 * 1024 + BUCKET_MAX * 12
+                                ? sort_smem_bytes(THREADS_SMALL)
+                                : THREADS_SMALL / 32 * 1024 + BUCKET_MAX * 12) +
+                           1024;
 
 // persistent CTAs, one instance each (k_solve_cta)
 struct CtaLaunch {
@@ -58,9 +68,28 @@ struct MaxIdLaunch {
 
 __device__ __forceinline__ Scratch make_scratch(char *base, uint64_t bytes) { return scratch_over(base, bytes); }
 
+// persistent CTAs: each pulls instances from the queue (largest first) and
+// solves them alone (BlockTeam)
+__device__ __forceinline__ void solve_queue_by_cta(const CtaLaunch &L, char *sm, int *next)
+{
+    BlockTeam t;
+    for (int guard = 0; guard < (1 << 30); ++guard) {
+        if (threadIdx.x == 0) *next = atomicAdd(L.queue, 1);
+        __syncthreads();
+        const int k = *next;
+        __syncthreads();
+        if (k >= L.count) break;
+        Instance *io = &L.inst[L.order[k]];
+        Scratch sc = make_scratch(io->ws, io->ws_bytes);
+        solve_instance(t, sm, sc, io);
+        __syncthreads();
+    }
+}
+
 }  // namespace rama
 
 __global__ void __launch_bounds__(rama::THREADS, 2) k_solve_cta(rama::CtaLaunch L);
+__global__ void __launch_bounds__(rama::THREADS_SMALL, 3) k_solve_cta_small(rama::CtaLaunch L);
 __global__ void __launch_bounds__(rama::THREADS, 2) k_solve_mixed(rama::MixedLaunch L);
 __global__ void __launch_bounds__(rama::THREADS, 2) k_solve_grid(rama::GridLaunch L);
 __global__ void __launch_bounds__(rama::THREADS, 2) k_parse_grid(rama::ParseLaunch L);

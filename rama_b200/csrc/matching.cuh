@@ -148,26 +148,40 @@ __device__ int32_t matching_contraction_map(const Team &t, Scratch &sc, char *sm
             const int64_t TILE = (int64_t)blockDim.x * MI;
             const int64_t wofs = (int64_t)warp_in_block() * 32 * MI;
             if (it == 0) {
+                // a lane takes MI = 4 consecutive edges: one 128-bit load per
+                // array when the arrays are 16-byte aligned (the graph slot is)
+                const bool vec = ((reinterpret_cast<uintptr_t>(A.row) | reinterpret_cast<uintptr_t>(A.col) |
+                                   reinterpret_cast<uintptr_t>(A.cost)) & 15) == 0;
                 for (int64_t tile = (int64_t)t.block() * TILE; tile < A.n; tile += (int64_t)t.nblocks() * TILE) {
                     int32_t u[MI], v[MI];
                     uint32_t hb[MI];
                     bool live[MI];
                     float c[MI];
+                    const int64_t e0 = tile + wofs + (int64_t)lane_id() * MI;
+                    if (vec && e0 + MI <= A.n) {
+                        const float4 c4 = *reinterpret_cast<const float4 *>(A.cost + e0);
+                        const int4 r4 = *reinterpret_cast<const int4 *>(A.row + e0);
+                        const int4 l4 = *reinterpret_cast<const int4 *>(A.col + e0);
+                        c[0] = c4.x, c[1] = c4.y, c[2] = c4.z, c[3] = c4.w;
+                        u[0] = r4.x, u[1] = r4.y, u[2] = r4.z, u[3] = r4.w;
+                        v[0] = l4.x, v[1] = l4.y, v[2] = l4.z, v[3] = l4.w;
 #pragma unroll
-                    for (int k = 0; k < MI; ++k) {
-                        const int64_t e = tile + wofs + k * 32 + lane_id();
-                        c[k] = e < A.n ? A.cost[e] : 0.0f;
+                        for (int k = 0; k < MI; ++k) live[k] = c[k] > thresh;
+                    } else {
+#pragma unroll
+                        for (int k = 0; k < MI; ++k) {
+                            const int64_t e = e0 + k;
+                            c[k] = e < A.n ? A.cost[e] : 0.0f;
+                            live[k] = e < A.n && c[k] > thresh;
+                            u[k] = live[k] ? A.row[e] : 0;
+                            v[k] = live[k] ? A.col[e] : 0;
+                        }
                     }
 #pragma unroll
                     for (int k = 0; k < MI; ++k) {
-                        const int64_t e = tile + wofs + k * 32 + lane_id();
-                        live[k] = e < A.n && c[k] > thresh;
-                        u[k] = live[k] ? A.row[e] : 0;
-                        v[k] = live[k] ? A.col[e] : 0;
                         hb[k] = float_ordered(c[k]);
+                        live[k] = live[k] && u[k] != v[k];
                     }
-#pragma unroll
-                    for (int k = 0; k < MI; ++k) live[k] = live[k] && u[k] != v[k];
                     offer_tile(u, v, hb, live);
                 }
             } else {

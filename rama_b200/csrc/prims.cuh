@@ -445,12 +445,20 @@ __device__ double team_csum_count(const Team &t, Scratch &sc, int64_t n, Get get
             csum_t a = {0.0, 0.0};
             int64_t c = 0;
             const int64_t b0 = ch * 4096 + lane_id();
-            for (int k = 0; k < 128; ++k) {
-                int64_t idx = b0 + 32 * k;
-                if (idx < n) {
-                    a = cs_merge(a, csum_t{get(idx), 0.0});
-                    c += cnt(idx) ? 1 : 0;
+            // 8 of the lane's 128 elements loaded at a time, merged in order
+            for (int k = 0; k < 128; k += 8) {
+                double x[8];
+                bool in[8];
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int64_t idx = b0 + 32 * (k + j);
+                    in[j] = idx < n;
+                    x[j] = in[j] ? get(idx) : 0.0;
+                    c += in[j] && cnt(idx) ? 1 : 0;
                 }
+#pragma unroll
+                for (int j = 0; j < 8; ++j)
+                    if (in[j]) a = cs_merge(a, csum_t{x[j], 0.0});
             }
             a = cs_warp_tree(a);
             c = warp_sum(c);
@@ -538,12 +546,22 @@ __device__ __forceinline__ float rsum_upto8(const float *p, int n)
     return (float)__dadd_rn(a, b);
 }
 
-// the same sum by a whole warp (any n); result valid on every lane
+// the same sum by a whole warp (any n); result valid on every lane.  Each
+// lane loads 8 of its elements at a time (independent loads in flight) and
+// adds them in order, so the sum is the lane-sequential one.
 template <class Get>
 __device__ __forceinline__ float rsum_warp(int64_t n, Get v)
 {
     double a = 0.0;
-    for (int64_t k = lane_id(); k < n; k += 32) a = __dadd_rn(a, (double)v(k));
+    int64_t k = lane_id();
+    for (; k + 32 * 7 < n; k += 32 * 8) {
+        float x[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) x[j] = v(k + 32 * j);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) a = __dadd_rn(a, (double)x[j]);
+    }
+    for (; k < n; k += 32) a = __dadd_rn(a, (double)v(k));
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
         double o = __shfl_down_sync(FULL, a, off);

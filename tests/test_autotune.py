@@ -74,3 +74,27 @@ def test_set_tuning_rejects_values_out_of_range():
     t.grid_ctas_per_sm = 0
     with pytest.raises(_lib.RamaError):
         s.handle.set_tuning(t)
+    t = s.handle.tuning()
+    t.cta_threads = 300
+    with pytest.raises(_lib.RamaError):
+        s.handle.set_tuning(t)
+
+
+@pytest.mark.gpu
+def test_small_cta_kernel_gives_the_same_batch_results():
+    """A batch without cluster instances on CTAs of 256 threads (three per SM)
+    and on CTAs of 512: the same labels and bounds."""
+    from rama_b200 import instances
+    from rama_b200.solver import Solver
+
+    b = instances.delaunay_batch(count=40, nmin=300, nmax=6000, seed=17)
+    s = Solver(0)
+    want, _, rc = s.solve_batch(b, mode="PD")
+    assert rc == 0
+    t = s.handle.tuning()
+    t.cta_threads, t.batch_cluster_min = 256, 1 << 40
+    s.handle.set_tuning(t)
+    got, _, rc = s.solve_batch(b, mode="PD")
+    assert rc == 0
+    for (lab, lb), (glab, glb) in zip(want, got):
+        assert np.array_equal(lab, glab) and lb == glb
