@@ -20,44 +20,28 @@ struct TriBuf {
     int none;       // no repulsive edge has an attractive edge at both ends: no cycle of any length
 };
 
-// The common neighbours of two sorted neighbour lists adj[a0, a1) and
-// adj[b0, b1), by a whole warp (warp-uniform arguments): lane l takes the
-// l-th element of each 32-element chunk of the first list and looks for it
-// in the second -- against a register copy of it (one element per lane,
-// compared through shuffles) when it has at most 32 elements, else by a
-// binary search of its own.  f(mid, j) is called by the lane that holds the
-// j-th common neighbour in ascending order; returns their number (on every
-// lane).  The lists have distinct entries (a simple graph).
-template <class F>
-__device__ __forceinline__ int warp_common(const int32_t *adj, int32_t a0, int32_t a1, int32_t b0, int32_t b1, F f)
+__device__ __forceinline__ int count_common(const int32_t *adj, int32_t a0, int32_t a1, int32_t b0, int32_t b1)
 {
-    const int lane = lane_id();
-    const int32_t nb = b1 - b0;
-    const bool small = nb <= 32;
-    const int32_t bv = small && lane < nb ? adj[b0 + lane] : -1;
-    int total = 0;
-    for (int32_t c = a0; c < a1; c += 32) {
-        const int32_t i = c + lane;
-        const int32_t x = i < a1 ? adj[i] : -2;
-        bool m = false;
-        if (small) {
-            for (int k = 0; k < nb; ++k) m |= __shfl_sync(FULL, bv, k) == x;
-        } else if (i < a1) {
-            int32_t lo = b0, hi = b1;
-            while (lo < hi) {
-                const int32_t mid = (lo + hi) >> 1;
-                if (adj[mid] < x)
-                    lo = mid + 1;
-                else
-                    hi = mid;
-            }
-            m = lo < b1 && adj[lo] == x;
-        }
-        const unsigned bal = __ballot_sync(FULL, m);
-        if (m) f(x, total + __popc(bal & lanemask_lt()));
-        total += __popc(bal);
+    int c = 0;
+    while (a0 < a1 && b0 < b1) {
+        int32_t x = adj[a0], y = adj[b0];
+        c += (x == y);
+        a0 += (x <= y);
+        b0 += (y <= x);
     }
-    return total;
+    return c;
+}
+
+// calls f(mid) for the common neighbours in ascending order while f returns true
+template <class F>
+__device__ __forceinline__ void for_common(const int32_t *adj, int32_t a0, int32_t a1, int32_t b0, int32_t b1, F f)
+{
+    while (a0 < a1 && b0 < b1) {
+        int32_t x = adj[a0], y = adj[b0];
+        if (x == y && !f(x)) return;
+        a0 += (x <= y);
+        b0 += (y <= x);
+    }
 }
 
 __device__ __forceinline__ void write_tri(TriBuf &tb, int64_t pos, int32_t a, int32_t b, int32_t c)
@@ -165,31 +149,8 @@ __device__ __forceinline__ int64_t expansion_owner(const int64_t *xo, int64_t R,
     return lo;
 }
 
-// Calls body(q, r, loc) for the expansions q of a chunk [x0, x0 + xn), one at
-// a time per warp: every warp takes a contiguous block of them, finds the
-// rep edge of its first one once and steps forward from there.
-template <class Team, class Body>
-__device__ __forceinline__ void for_expansions_by_warp(const Team &t, const int64_t *xo, int64_t R, int64_t x0,
-                                                       int64_t xn, Body body)
-{
-    const int64_t nw = team_nwarps(t), w = team_warp(t);
-    const int64_t per = (xn + nw - 1) / nw;
-    const int64_t q0 = w * per, q1 = q0 + per < xn ? q0 + per : xn;
-    if (q0 >= q1) return;
-    int64_t r = expansion_owner(xo, R, x0 + q0);
-    for (int64_t q = q0; q < q1; ++q) {
-        const int64_t x = x0 + q;
-        if (xo)
-            while (r < R && xo[r + 1] <= x) ++r;
-        else
-            r = x;
-        body(q, r, xo ? x - xo[r] : 0);
-    }
-}
-
-// cnt(r, loc) and emit(r, loc, pos, keep) are called by a whole warp for one
-// expansion: cnt returns its number of emissions (on every lane), emit writes
-// the first `keep` of them at pos, pos + 1, ...
+// emit(r, loc, pos, keep) writes the first `keep` emissions of an expansion
+// at pos, pos + 1, ...
 template <class Team, class Count, class Emit>
 __device__ void expansion_stage(const Team &t, Scratch &sc, char *sm, TriBuf &tb, const int64_t *xo, int64_t R,
                                 int64_t X, Count cnt, Emit emit)
@@ -202,11 +163,23 @@ __device__ void expansion_stage(const Team &t, Scratch &sc, char *sm, TriBuf &tb
     if (!sc.arena.ok()) return;
     for (int64_t x0 = 0; x0 < X && tb.count <= tb.budget; x0 += CH) {
         const int64_t xn = (X - x0) < CH ? (X - x0) : CH;
-        // count (a warp per expansion)
-        for_expansions_by_warp(t, xo, R, x0, xn, [&](int64_t q, int64_t r, int64_t loc) {
-            const int c = cnt(r, loc);
-            if (lane_id() == 0) ccount[q] = c;
-        });
+        // count
+        // a warp takes 32 consecutive expansions: one search for the owner of
+        // the first, then each lane steps forward to its own
+        for (int64_t qb = (int64_t)team_warp(t) * 32; qb < xn; qb += (int64_t)team_nwarps(t) * 32) {
+            int64_t r0 = lane_id() == 0 ? expansion_owner(xo, R, x0 + qb) : 0;
+            r0 = __shfl_sync(FULL, r0, 0);
+            const int64_t q = qb + lane_id();
+            if (q >= xn) continue;
+            const int64_t x = x0 + q;
+            int64_t r = xo ? r0 : x;
+            if (xo) {
+                int steps = 0;  // long runs of rep edges without expansions: search instead
+                while (r < R && xo[r + 1] <= x && ++steps <= 64) ++r;
+                if (steps > 64) r = expansion_owner(xo, R, x);
+            }
+            ccount[q] = cnt(r, xo ? x - xo[r] : 0);
+        }
         t.sync();
         const int64_t start = tb.count;
         const int64_t rem = tb.budget - start;
@@ -246,10 +219,22 @@ __device__ void expansion_stage(const Team &t, Scratch &sc, char *sm, TriBuf &tb
                 cbase[q] = pmin + (pbig < extra ? pbig : extra);
                 ccount[q] = (int32_t)((v >> 25) + ((v & 1) && pbig < extra ? 1 : 0));
             });
-        for_expansions_by_warp(t, xo, R, x0, xn, [&](int64_t q, int64_t r, int64_t loc) {
-            const int32_t keep = ccount[q];
-            if (keep) emit(r, loc, start + cbase[q], (int64_t)keep);
-        });
+        for (int64_t qb = (int64_t)team_warp(t) * 32; qb < xn; qb += (int64_t)team_nwarps(t) * 32) {
+            const int64_t q = qb + lane_id();
+            const bool work = q < xn && ccount[q] != 0;
+            if (!__any_sync(FULL, work)) continue;
+            int64_t r0 = lane_id() == 0 ? expansion_owner(xo, R, x0 + qb) : 0;
+            r0 = __shfl_sync(FULL, r0, 0);
+            if (!work) continue;
+            const int64_t x = x0 + q;
+            int64_t r = xo ? r0 : x;
+            if (xo) {
+                int steps = 0;  // long runs of rep edges without expansions: search instead
+                while (r < R && xo[r + 1] <= x && ++steps <= 64) ++r;
+                if (steps > 64) r = expansion_owner(xo, R, x);
+            }
+            emit(r, xo ? x - xo[r] : 0, start + cbase[q], (int64_t)ccount[q]);
+        }
         t.sync();
         tb.count = tot <= rem ? start + tot : tb.budget + 1;
     }
@@ -331,13 +316,15 @@ __device__ void conflicted_cycles(const Team &t, Scratch &sc, char *sm, const Gr
         expansion_stage(
             t, sc, sm, T, nullptr, R, R,
             [&](int64_t r, int64_t) {
-                const int32_t v1 = rv1(r), v2 = rv2(r);
-                return warp_common(adj, off[v1], off[v1 + 1], off[v2], off[v2 + 1], [](int32_t, int) {});
+                int32_t v1 = rv1(r), v2 = rv2(r);
+                return count_common(adj, off[v1], off[v1 + 1], off[v2], off[v2 + 1]);
             },
             [&](int64_t r, int64_t, int64_t pos, int64_t keep) {
-                const int32_t v1 = rv1(r), v2 = rv2(r);
-                warp_common(adj, off[v1], off[v1 + 1], off[v2], off[v2 + 1], [&](int32_t mid, int j) {
-                    if (j < keep) write_tri(T, pos + j, v1, v2, mid);
+                int32_t v1 = rv1(r), v2 = rv2(r);
+                int64_t e = 0;
+                for_common(adj, off[v1], off[v1 + 1], off[v2], off[v2 + 1], [&](int32_t mid) {
+                    write_tri(T, pos + e, v1, v2, mid);
+                    return ++e < keep;
                 });
             });
     }
@@ -353,17 +340,19 @@ __device__ void conflicted_cycles(const Team &t, Scratch &sc, char *sm, const Gr
         expansion_stage(
             t, sc, sm, T, xo, R, X,
             [&](int64_t r, int64_t loc) {
-                const int32_t v2 = rv2(r);
-                const int32_t n1 = adj[off[rv1(r)] + loc];
-                return 2 * warp_common(adj, off[n1], off[n1 + 1], off[v2], off[v2 + 1], [](int32_t, int) {});
+                int32_t v1 = rv1(r), v2 = rv2(r);
+                int32_t n1 = adj[off[v1] + loc];
+                return 2 * count_common(adj, off[n1], off[n1 + 1], off[v2], off[v2 + 1]);
             },
             [&](int64_t r, int64_t loc, int64_t pos, int64_t keep) {
-                const int32_t v1 = rv1(r), v2 = rv2(r);
-                const int32_t n1 = adj[off[v1] + loc];
-                warp_common(adj, off[n1], off[n1 + 1], off[v2], off[v2 + 1], [&](int32_t mid, int j) {
-                    const int64_t e = 2 * (int64_t)j;
-                    if (e < keep) write_tri(T, pos + e, v1, v2, n1);
-                    if (e + 1 < keep) write_tri(T, pos + e + 1, v2, n1, mid);
+                int32_t v1 = rv1(r), v2 = rv2(r);
+                int32_t n1 = adj[off[v1] + loc];
+                int64_t e = 0;
+                for_common(adj, off[n1], off[n1 + 1], off[v2], off[v2 + 1], [&](int32_t mid) {
+                    write_tri(T, pos + e, v1, v2, n1);
+                    if (++e >= keep) return false;
+                    write_tri(T, pos + e, v2, n1, mid);
+                    return ++e < keep;
                 });
             });
     }
@@ -383,24 +372,27 @@ __device__ void conflicted_cycles(const Team &t, Scratch &sc, char *sm, const Gr
         expansion_stage(
             t, sc, sm, T, xo, R, X,
             [&](int64_t r, int64_t loc) {
-                const int32_t v1 = rv1(r), v2 = rv2(r);
-                const int64_t d1 = off[v1 + 1] - off[v1];
-                const int32_t n1 = adj[off[v1] + (int32_t)(loc % d1)];
-                const int32_t n2 = adj[off[v2] + (int32_t)(loc / d1)];
+                int32_t v1 = rv1(r), v2 = rv2(r);
+                int64_t d1 = off[v1 + 1] - off[v1];
+                int32_t n1 = adj[off[v1] + (int32_t)(loc % d1)];
+                int32_t n2 = adj[off[v2] + (int32_t)(loc / d1)];
                 if (n1 == n2) return 0;
-                return 3 * warp_common(adj, off[n1], off[n1 + 1], off[n2], off[n2 + 1], [](int32_t, int) {});
+                return 3 * count_common(adj, off[n1], off[n1 + 1], off[n2], off[n2 + 1]);
             },
             [&](int64_t r, int64_t loc, int64_t pos, int64_t keep) {
-                const int32_t v1 = rv1(r), v2 = rv2(r);
-                const int64_t d1 = off[v1 + 1] - off[v1];
-                const int32_t n1 = adj[off[v1] + (int32_t)(loc % d1)];
-                const int32_t n2 = adj[off[v2] + (int32_t)(loc / d1)];
+                int32_t v1 = rv1(r), v2 = rv2(r);
+                int64_t d1 = off[v1 + 1] - off[v1];
+                int32_t n1 = adj[off[v1] + (int32_t)(loc % d1)];
+                int32_t n2 = adj[off[v2] + (int32_t)(loc / d1)];
                 if (n1 == n2) return;
-                warp_common(adj, off[n1], off[n1 + 1], off[n2], off[n2 + 1], [&](int32_t mid, int j) {
-                    const int64_t e = 3 * (int64_t)j;
-                    if (e < keep) write_tri(T, pos + e, v1, v2, n1);
-                    if (e + 1 < keep) write_tri(T, pos + e + 1, v2, n1, mid);
-                    if (e + 2 < keep) write_tri(T, pos + e + 2, v2, mid, n2);
+                int64_t e = 0;
+                for_common(adj, off[n1], off[n1 + 1], off[n2], off[n2 + 1], [&](int32_t mid) {
+                    write_tri(T, pos + e, v1, v2, n1);
+                    if (++e >= keep) return false;
+                    write_tri(T, pos + e, v2, n1, mid);
+                    if (++e >= keep) return false;
+                    write_tri(T, pos + e, v2, mid, n2);
+                    return ++e < keep;
                 });
             });
     }

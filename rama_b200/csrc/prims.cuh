@@ -546,22 +546,12 @@ __device__ __forceinline__ float rsum_upto8(const float *p, int n)
     return (float)__dadd_rn(a, b);
 }
 
-// the same sum by a whole warp (any n); result valid on every lane.  Each
-// lane loads 8 of its elements at a time (independent loads in flight) and
-// adds them in order, so the sum is the lane-sequential one.
+// the same sum by a whole warp (any n); result valid on every lane
 template <class Get>
 __device__ __forceinline__ float rsum_warp(int64_t n, Get v)
 {
     double a = 0.0;
-    int64_t k = lane_id();
-    for (; k + 32 * 7 < n; k += 32 * 8) {
-        float x[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) x[j] = v(k + 32 * j);
-#pragma unroll
-        for (int j = 0; j < 8; ++j) a = __dadd_rn(a, (double)x[j]);
-    }
-    for (; k < n; k += 32) a = __dadd_rn(a, (double)v(k));
+    for (int64_t k = lane_id(); k < n; k += 32) a = __dadd_rn(a, (double)v(k));
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
         double o = __shfl_down_sync(FULL, a, off);
