@@ -322,7 +322,27 @@ def phase_roofline(stats, hbm):
             continue
         gbs = b / (ms / 1e3) / 1e9 if ms > 0 else 0.0
         out[name] = {"ms": round(ms, 3), "bytes": b, "gbs": round(gbs, 1), "frac": round(gbs / hbm, 4)}
+    # a step's bytes are tallied where the step ends, its time in the
+    # sub-phases it marks: the steps as a whole carry the meaningful rates
+    groups = {}
+    for step, parts in PHASE_GROUPS.items():
+        ms = sum(out[p]["ms"] for p in parts if p in out)
+        b = sum(out[p]["bytes"] for p in parts if p in out)
+        if ms > 0:
+            gbs = b / (ms / 1e3) / 1e9
+            groups[step] = {"ms": round(ms, 3), "bytes": b, "gbs": round(gbs, 1), "frac": round(gbs / hbm, 4)}
+    out["steps"] = groups
     return out
+
+
+PHASE_GROUPS = {
+    "init": ("init",),
+    "cycle search": ("cycles", "csr", "cyc_search"),
+    "message passing": ("mp_norm", "mp_chords", "mp_incid", "mp_build", "mp_iter", "dual_commit"),
+    "matching": ("matching", "match_first", "match_iter", "match_labels"),
+    "forest": ("woc_msf", "woc_csr", "woc_checks", "woc_root", "woc_paths", "woc"),
+    "contraction": ("contract", "csort_big", "csort_slot", "csort_scatter", "csort_rank", "contract_runs"),
+}
 
 
 def tune_solver(s, device, args):

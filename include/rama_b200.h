@@ -87,12 +87,19 @@ typedef struct {
     double device_ms;        /* kernel time of the solve (CUDA events) */
     double alg_bytes;        /* algorithmic bytes of the solve: minimum edge, map, arc and triangle
                                 traffic of each phase, tallied on the device; no sort temporaries */
-    double phase_ms[16];     /* time per phase: init, cycle search, MP build, MP iterations + bound,
-                                dual commit, matching (threshold, labels), forest contraction set,
-                                contraction (after its sort), other, matching iterations, contraction
-                                sort of buckets beyond 4096 edges, CSR builds, contraction sort
-                                (endpoints and slots, scatter, ordering in buckets), contraction runs */
-    double phase_bytes[16];  /* algorithmic bytes per phase (same order), the parts of alg_bytes */
+    double phase_ms[32];     /* time per phase: [0] init, [1] cycle search (classification),
+                                [2] MP build (rest), [3] MP iterations + bound, [4] dual commit,
+                                [5] matching (threshold), [6] forest contraction set (rest),
+                                [7] contraction (after its sort), [8] other, [9] matching iterations
+                                after the first, [10] contraction sort of buckets beyond 4096 edges,
+                                [11] CSR builds, [12..14] contraction sort (endpoints and slots,
+                                scatter, ordering in buckets), [15] contraction runs, [16] matching
+                                labels, [17] first matching iteration, [18] forest MSF, [19] forest
+                                lists, [20] forest components / checks / thresholds, [21] forest
+                                rooting, [22] forest path lengths and cuts, [23] cycle expansions,
+                                [24] triangle normalisation, [25] MP chords and merged edges,
+                                [26] MP correspondence and incidence order; [27..31] unused */
+    double phase_bytes[32];  /* algorithmic bytes per phase (same order), the parts of alg_bytes */
 } rama_stats;
 
 /*
@@ -247,7 +254,9 @@ enum {
     RAMA_STEP_MP = 8,         /* graph + triangles -> lb0, lb1, reparametrised edges (multicut_message_passing.cu) */
     RAMA_STEP_DUAL = 9,       /* graph -> lb, reparametrised graph   dual_solver.cu:37-63 */
     RAMA_STEP_CSUM = 10,      /* float array -> compensated sum */
-    RAMA_STEP_SORT = 11       /* (uint64 key, int32 value) pairs -> stable sorted */
+    RAMA_STEP_SORT = 11,      /* (uint64 key, int32 value) pairs -> stable sorted */
+    RAMA_STEP_COARSEN = 12    /* graph + map -> the solver's contraction: contract_cuda, has_bad_contractions
+                                 and remove_diagonal (src/dCOO.cu:57-152); out_nr = 1 on a bad contraction */
 };
 
 typedef struct {

@@ -189,26 +189,52 @@ double orc_csum_f32(const float *x, int64_t n)
     return cacc_finish(&a);
 }
 
-/* C3: RSUM, plain FP64 lane-strided sums + pairwise tree, rounded to float */
+/* C3: RSUM, plain FP64 lane-strided sums + pairwise tree, rounded to float.
+ * Up to 4096 values: value k goes to lane k mod 32 (each lane starts at +0.0
+ * and adds its values in order), then a pairwise tree over the 32 lanes.
+ * More than 4096 values: each chunk of 4096 consecutive values is summed that
+ * way (kept in double), and the chunk sums are summed the same way (chunk c
+ * to lane c mod 32), so that many warps can share one long sum on the GPU. */
 typedef struct {
     double lane[32];
+    double chunk_lane[32];
     int64_t idx;
+    int64_t chunks;
 } rsum_acc;
+static inline double racc_tree(double *lane)
+{
+    for (int off = 1; off < 32; off *= 2)
+        for (int l = 0; l < 32; l += 2 * off) lane[l] = lane[l] + lane[l + off];
+    return lane[0];
+}
 static inline void racc_init(rsum_acc *a)
 {
     memset(a->lane, 0, sizeof(a->lane));
+    memset(a->chunk_lane, 0, sizeof(a->chunk_lane));
     a->idx = 0;
+    a->chunks = 0;
 }
 static inline void racc_push(rsum_acc *a, float x)
 {
     a->lane[a->idx & 31] += (double)x;
     a->idx++;
+    if ((a->idx & 4095) == 0) {
+        a->chunk_lane[a->chunks & 31] += racc_tree(a->lane);
+        a->chunks++;
+        memset(a->lane, 0, sizeof(a->lane));
+    }
 }
 static inline float racc_finish(rsum_acc *a)
 {
-    for (int off = 1; off < 32; off *= 2)
-        for (int l = 0; l < 32; l += 2 * off) a->lane[l] = a->lane[l] + a->lane[l + off];
-    return (float)a->lane[0];
+    if (a->idx <= 4096) {
+        if (a->chunks == 1) return (float)a->chunk_lane[0]; /* exactly 4096 values */
+        return (float)racc_tree(a->lane);
+    }
+    if ((a->idx & 4095) != 0) {
+        a->chunk_lane[a->chunks & 31] += racc_tree(a->lane);
+        a->chunks++;
+    }
+    return (float)racc_tree(a->chunk_lane);
 }
 
 float orc_rsum_f32(const float *x, int64_t n)

@@ -20,7 +20,8 @@ RAMA_ERR_CUDA = 3
 RAMA_ERR_ITER_LIMIT = 4
 RAMA_ERR_BAD_CONTRACTION = 5
 
-STEP = dict(INIT=1, CONTRACT=2, MATCHING=3, WOC=4, MSF=5, CC=6, CYCLES=7, MP=8, DUAL=9, CSUM=10, SORT=11)
+STEP = dict(INIT=1, CONTRACT=2, MATCHING=3, WOC=4, MSF=5, CC=6, CYCLES=7, MP=8, DUAL=9, CSUM=10, SORT=11,
+            COARSEN=12)
 
 
 class RamaOptions(C.Structure):
@@ -56,8 +57,8 @@ class RamaStats(C.Structure):
         ("workspace_peak", C.c_int64),
         ("device_ms", C.c_double),
         ("alg_bytes", C.c_double),
-        ("phase_ms", C.c_double * 16),
-        ("phase_bytes", C.c_double * 16),
+        ("phase_ms", C.c_double * 32),
+        ("phase_bytes", C.c_double * 32),
     ]
 
 class RamaTuning(C.Structure):
@@ -78,7 +79,9 @@ class RamaTuning(C.Structure):
 
 
 PHASES = ("init", "cycles", "mp_build", "mp_iter", "dual_commit", "matching", "woc", "contract", "other",
-          "match_iter", "csort_big", "csr", "csort_slot", "csort_scatter", "csort_rank", "contract_runs")
+          "match_iter", "csort_big", "csr", "csort_slot", "csort_scatter", "csort_rank", "contract_runs",
+          "match_labels", "match_first", "woc_msf", "woc_csr", "woc_checks", "woc_root", "woc_paths",
+          "cyc_search", "mp_norm", "mp_chords", "mp_incid", "-", "-", "-", "-", "-")
 
 
 _P = C.c_void_p

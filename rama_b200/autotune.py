@@ -11,7 +11,9 @@ built-in choices are guesses; this module measures them on the device:
   the whole-GPU solve, for large graphs and for graphs below a size (fewer
   CTAs take cheaper grid barriers, more CTAs hide more memory latency), timed
   on 3-D grids of growing size;
-* cluster_ctas: the cluster size, timed on mid-size Delaunay graphs;
+* cluster_ctas: the cluster size, timed on mid-size Delaunay graphs, and
+  again (against the built-in size) inside the batch trial below, which has
+  the last word: a batch runs many clusters side by side;
 * single_cluster_min / single_grid_min: where a single solve moves from one
   CTA to a cluster and from a cluster to the whole GPU -- each team is timed
   on graphs of increasing size and the switch goes to the first size at which
@@ -19,7 +21,7 @@ built-in choices are guesses; this module measures them on the device:
 * batch_cluster_min / batch_cluster_share / cta_threads: which instances of
   a batch get a cluster, and whether the instances solved alone take CTAs of
   512 threads (two per SM) or 256 (three per SM), timed together on a batch
-  of Delaunay graphs of uneven size.
+  of 256 Delaunay graphs of uneven size.
 
 Every trial solve's labels and bound are checked to equal the first trial's:
 a tuning never changes a result, and the tuner fails loudly if one would.
@@ -240,20 +242,27 @@ def tune(device: int = 0, budget_s: float = 60.0, quick: bool = False) -> dict:
     tables["single"] = {"edges": sizes, "cta_ms": cta, "cluster_ms": clu, "grid_ms": grd}
     tr.set(**chosen)
 
-    # batches: which instances get a cluster
-    batch = I.delaunay_batch(count=96 if not quick else 24, nmin=500, nmax=20000, seed=11)
-    # (and the CTA size of the instances that run alone: a batch without
-    # cluster instances runs on the per-instance CTA kernel of that size)
+    # batches: which instances get a cluster, on a batch large enough that
+    # many clusters and CTAs run side by side (the cluster size that is best
+    # for one solve alone need not be best there: both are tried, and the
+    # batch decides); and the CTA size of the instances that run alone (a
+    # batch without cluster instances runs on the per-instance CTA kernel of
+    # that size)
+    batch = I.delaunay_batch(count=256 if not quick else 24, nmin=500, nmax=20000, seed=11)
+    csizes = [chosen["cluster_ctas"]] + [c for c in tc if c != chosen["cluster_ctas"] and c == base["cluster_ctas"]]
     tb = {}
-    for threads in (512, 256):
-        for bmin, share in ((10000, 1.0), (20000, 1.5), (20000, 3.0), (40000, 1.5), (1 << 40, 1.5)):
-            if time.perf_counter() - t0 > budget_s and tb:
-                break
-            tr.set(**{**chosen, "batch_cluster_min": bmin, "batch_cluster_share": share, "cta_threads": threads})
-            tb[(bmin, share, threads)] = tr.batch("batch", batch, "PD")
-    bmin, share, threads = pick_fastest(tb)
+    for csz in csizes:
+        for threads in (512, 256):
+            for bmin, share in ((10000, 1.0), (20000, 1.5), (20000, 3.0), (40000, 1.5), (1 << 40, 1.5)):
+                if time.perf_counter() - t0 > budget_s and tb:
+                    break
+                tr.set(**{**chosen, "cluster_ctas": csz, "batch_cluster_min": bmin, "batch_cluster_share": share,
+                          "cta_threads": threads})
+                tb[(bmin, share, threads, csz)] = tr.batch("batch", batch, "PD")
+    bmin, share, threads, csz = pick_fastest(tb)
     chosen["batch_cluster_min"], chosen["batch_cluster_share"], chosen["cta_threads"] = bmin, share, threads
-    tables["batch"] = {f"{k[0]}/{k[1]}/{k[2]}": v for k, v in tb.items()}
+    chosen["cluster_ctas"] = csz
+    tables["batch"] = {f"{k[0]}/{k[1]}/{k[2]}/{k[3]}": v for k, v in tb.items()}
     tr.set(**chosen)
     return {"tuning": chosen, "default": base, "tables": tables, "seconds": round(time.perf_counter() - t0, 1)}
 

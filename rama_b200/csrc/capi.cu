@@ -357,7 +357,7 @@ int solve_one(rama_context *h, const int32_t *d_i, const int32_t *d_j, const flo
         {
             int64_t pr[2 * PH_COUNT];
             CU(cudaMemcpy(pr, h->d_prof, sizeof(pr), cudaMemcpyDeviceToHost));
-            for (int k = 0; k < PH_COUNT && k < 16; ++k) {
+            for (int k = 0; k < PH_COUNT && k < 32; ++k) {
                 h->stats.phase_ms[k] = 1e-6 * (double)pr[k];
                 h->stats.phase_bytes[k] = (double)pr[PH_COUNT + k];
             }

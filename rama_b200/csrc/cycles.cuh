@@ -270,12 +270,40 @@ __device__ void conflicted_cycles(const Team &t, Scratch &sc, char *sm, const Gr
     if (!sc.arena.ok()) return;
     for (int64_t v = t.rank(); v < N; v += t.size()) haspos[v] = 0;
     t.sync();
-    const int64_t P = team_sum<Team, int64_t>(t, sc, sm, A.n, [&](int64_t e) -> int64_t {
-        if (!(A.cost[e] > pos_tol)) return 0;
-        haspos[A.row[e]] = 1;
-        haspos[A.col[e]] = 1;
-        return 1;
-    });
+    int64_t pc = 0;
+    {
+        // four edges a thread at a time: costs, then the ends of the
+        // attractive ones, then the marks
+        constexpr int U = 4;
+        const int64_t S = t.size();
+        int64_t e0 = t.rank();
+        for (; e0 + (U - 1) * S < A.n; e0 += U * S) {
+            float c[U];
+            int32_t a[U], b[U];
+#pragma unroll
+            for (int k = 0; k < U; ++k) c[k] = A.cost[e0 + k * S];
+#pragma unroll
+            for (int k = 0; k < U; ++k)
+                if (c[k] > pos_tol) {
+                    a[k] = A.row[e0 + k * S];
+                    b[k] = A.col[e0 + k * S];
+                }
+#pragma unroll
+            for (int k = 0; k < U; ++k)
+                if (c[k] > pos_tol) {
+                    haspos[a[k]] = 1;
+                    haspos[b[k]] = 1;
+                    ++pc;
+                }
+        }
+        for (; e0 < A.n; e0 += S)
+            if (A.cost[e0] > pos_tol) {
+                haspos[A.row[e0]] = 1;
+                haspos[A.col[e0]] = 1;
+                ++pc;
+            }
+    }
+    const int64_t P = team_total<Team, int64_t>(t, sc, sm, pc);
     // one pass counts both: the low 32 bits count every repulsive edge (the
     // budget counts them all, :247), the high bits the kept ones; the kept
     // ones are compacted only when there are any
@@ -289,6 +317,7 @@ __device__ void conflicted_cycles(const Team &t, Scratch &sc, char *sm, const Gr
     sc.alg_bytes += 12.0 * (double)A.n;
     if (P == 0 || R == 0) {
         tb.none = 1;
+        prof_mark(t, sc, PH_CYCLES);
         return;
     }
     team_scan<Team, int64_t>(

@@ -119,17 +119,16 @@ __device__ Graph graph_from_edges(const Team &t, Scratch &sc, char *sm, const in
     if (!sc.arena.ok()) return out;
     const bool done = team_bucket_sort_ex(
         t, sc, sm, n, mx + 1,
-        [&](int64_t e) {
+        [&](int64_t e) -> int64_t {
             const int32_t a = i[e], b = j[e];
             const int32_t lo = a < b ? a : b, hi = a < b ? b : a;
-            lohi[e] = make_int2(lo, hi);
-            return lo;
+            return ((int64_t)hi << 32) | (uint32_t)lo;
         },
         [&](int64_t e) { return lohi[e].x; },
         [&](int64_t e) -> uint64_t { return ((uint64_t)(uint32_t)lohi[e].y << 32) | (uint64_t)e; },
         [&](int64_t e) { return __float_as_int(c[e]); }, sk, sbits, bst, sbk, -1,
         [&](int64_t e) -> uint64_t { return ((uint64_t)(uint32_t)lohi[e].x << nbh) | (uint32_t)lohi[e].y; },
-        2 * nbh);
+        2 * nbh, [&](int64_t e, int64_t w) { lohi[e] = make_int2((int32_t)(uint32_t)w, (int32_t)(w >> 32)); });
     if (!done) return out;
     Arena &ar = sc.arena;
     const uint64_t bytes = (uint64_t)(n + 1) * 12 + 3 * 256;
@@ -144,11 +143,13 @@ __device__ Graph graph_from_edges(const Team &t, Scratch &sc, char *sm, const in
     g.col = reinterpret_cast<int32_t *>(ar.base + top + words);
     g.cost = reinterpret_cast<float *>(ar.base + top + 2 * words);
     g.n = n;
-    for (int64_t p = t.rank(); p < n; p += t.size()) {
-        g.row[p] = sbk[p];
-        g.col[p] = (int32_t)(sk[p] >> 32);
-        g.cost[p] = __int_as_float(sbits[p]);
-    }
+    team_for_batched(
+        t, n, [&](int64_t p) { return make_int3(sbk[p], (int32_t)(sk[p] >> 32), sbits[p]); },
+        [&](int64_t p, int3 v) {
+            g.row[p] = v.x;
+            g.col[p] = v.y;
+            g.cost[p] = __int_as_float(v.z);
+        });
     t.sync();
     graph_set_dims(t, sc, sm, g);
     ar.top = top;
@@ -390,17 +391,16 @@ __device__ Graph graph_contract(const Team &t, Scratch &sc, char *sm, const Grap
     }
     const bool done = team_bucket_sort_ex(
         t, sc, sm, n, nbk,
-        [&](int64_t e) {
+        [&](int64_t e) -> int64_t {
             const int32_t a = map[A.row[e]], b = map[A.col[e]];
             const int32_t lo = a < b ? a : b, hi = a < b ? b : a;
-            lohi[e] = make_int2(lo, hi);
-            return lo;
+            return ((int64_t)hi << 32) | (uint32_t)lo;
         },
         [&](int64_t e) { return lohi[e].x; },
         [&](int64_t e) -> uint64_t { return ((uint64_t)(uint32_t)lohi[e].y << 32) | (uint64_t)e; },
         [&](int64_t e) { return __float_as_int(A.cost[e]); }, sk, sbits, bst, sbk, PH_CSORT_SLOT,
         [&](int64_t e) -> uint64_t { return ((uint64_t)(uint32_t)lohi[e].x << nbh) | (uint32_t)lohi[e].y; },
-        2 * nbh);
+        2 * nbh, [&](int64_t e, int64_t w) { lohi[e] = make_int2((int32_t)(uint32_t)w, (int32_t)(w >> 32)); });
     if (!done) {
         sc.arena.release(m);
         return graph_contract_sorted(t, sc, sm, A, map, map_max, bad);
@@ -414,19 +414,30 @@ __device__ Graph graph_contract(const Team &t, Scratch &sc, char *sm, const Grap
         ar.failed = 1;
         return out;
     }
+    // temporaries taken from here on stay below the new slot (when the old
+    // graph does not live in the slot, as in a single step, the arena's top
+    // is its end)
+    if (top < ar.top) ar.top = top;
     const uint64_t words = ((uint64_t)(n + 1) * 4 + 255) / 256 * 256;
     Graph h;
     h.row = reinterpret_cast<int32_t *>(ar.base + top);
     h.col = reinterpret_cast<int32_t *>(ar.base + top + words);
     h.cost = reinterpret_cast<float *>(ar.base + top + 2 * words);
     // 3. heads of the runs: one scan counts every run (high 32 bits) and the
-    //    runs that are not self-loops (low 32 bits); the head's thread sums a
-    //    run of at most 32 edges, a longer run goes to a warp, which finds its
-    //    end at the next run's head
+    //    runs that are not self-loops (low 32 bits), writes the row and column
+    //    of each new edge and notes each run's start and output slot (-1: a
+    //    self-loop).  Then a pass over the runs sums each one, its end being
+    //    the next run's start: runs of up to 32 edges by one thread, longer
+    //    ones by a warp afterwards.
     auto head = [&](int64_t p) {
         return p == 0 || sbk[p] != sbk[p - 1] || (sk[p] >> 32) != (sk[p - 1] >> 32);
     };
-    int32_t *runstart = reinterpret_cast<int32_t *>(lohi);  // lohi is dead after the sort
+    // lohi is dead after the sort: its two halves hold the runs' starts and slots
+    int32_t *runstart = reinterpret_cast<int32_t *>(lohi);
+    int32_t *runk = runstart + (n + 1);
+    // the largest self-loop column, per thread first: one atomic per warp
+    // afterwards instead of one per self-loop run on a single word
+    int32_t dloc = -1;
     const int64_t packed = team_scan<Team, int64_t>(
         t, sc, sm, n,
         [&](int64_t p) -> int64_t {
@@ -436,51 +447,122 @@ __device__ Graph graph_contract(const Team &t, Scratch &sc, char *sm, const Grap
         [&](int64_t p, int64_t pre, int64_t v) {
             if (!v) return;
             const int64_t k = pre & 0xffffffffll, r = pre >> 32;
-            const bool nondiag = (v & 1) != 0;
-            runstart[r] = (int32_t)p;
             const int32_t b = sbk[p], hi = (int32_t)(sk[p] >> 32);
-            int64_t q = p + 1;
-            while (q < n && q - p <= 32 && sbk[q] == b && (int32_t)(sk[q] >> 32) == hi) ++q;
-            if (q - p <= 32) {
-                const int32_t len = (int32_t)(q - p);
-                const float sum =
-                    len <= RSUM_THREAD_MAX
-                        ? rsum_upto8(reinterpret_cast<const float *>(sbits + p), len)
-                        : rsum_serial(len, [&](int x) { return __int_as_float(sbits[p + x]); });
-                if (nondiag) {
-                    h.row[k] = b;
-                    h.col[k] = hi;
-                    h.cost[k] = sum;
-                } else {
-                    atomicMax(&fl[2], hi);
-                    if (sum < 0.0f) fl[0] = 1;
-                }
+            runstart[r] = (int32_t)p;
+            if (v & 1) {
+                runk[r] = (int32_t)k;
+                h.row[k] = b;
+                h.col[k] = hi;
             } else {
-                const int32_t slot = atomicAdd(&fl[1], 1);
-                longq[slot] = make_int4((int32_t)p, (int32_t)r, nondiag ? (int32_t)k : -1, hi);
-                if (nondiag) {
-                    h.row[k] = b;
-                    h.col[k] = hi;
-                } else {
-                    atomicMax(&fl[2], hi);
-                }
+                runk[r] = -1;
+                dloc = hi > dloc ? hi : dloc;
             }
         });
     const int64_t nk = packed & 0xffffffffll, nruns = packed >> 32;
-    const int32_t nl = uread(&fl[1]);
-    for (int64_t w = team_warp(t); w < nl; w += team_nwarps(t)) {
-        const int4 L = longq[w];
-        const int64_t end = L.y + 1 < nruns ? (int64_t)runstart[L.y + 1] : n;
-        const float v = rsum_warp(end - L.x, [&](int64_t x) { return __int_as_float(sbits[L.x + x]); });
-        if (lane_id() == 0) {
-            if (L.z < 0) {
-                if (v < 0.0f) fl[0] = 1;
-            } else {
-                h.cost[L.z] = v;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        const int32_t x = __shfl_xor_sync(FULL, dloc, o);
+        dloc = x > dloc ? x : dloc;
+    }
+    if (lane_id() == 0 && dloc >= 0) atomicMax(&fl[2], dloc);
+    const float *cost_sorted = reinterpret_cast<const float *>(sbits);
+    // a run's sum goes to its edge; a self-loop's negative sum is a bad contraction
+    auto finish = [&](int32_t k, float sum) {
+        if (k >= 0)
+            h.cost[k] = sum;
+        else if (sum < 0.0f)
+            fl[0] = 1;
+    };
+    {
+        // four runs a thread at a time: starts and slots, then the sums
+        constexpr int U = 4;
+        const int64_t S = t.size();
+        int64_t r0 = t.rank();
+        auto one = [&](int64_t r, int32_t s, int32_t e, int32_t k) {
+            const int32_t len = e - s;
+            if (len <= RSUM_THREAD_MAX)
+                finish(k, rsum_upto8(cost_sorted + s, len));
+            else if (len <= 32)
+                finish(k, rsum_upto32(cost_sorted + s, len));
+            else
+                longq[atomicAdd(&fl[1], 1)] = make_int4(s, e, k, 0);
+        };
+        for (; r0 + (U - 1) * S < nruns; r0 += U * S) {
+            int32_t s[U], e[U], k[U];
+#pragma unroll
+            for (int j = 0; j < U; ++j) {
+                const int64_t r = r0 + j * S;
+                s[j] = runstart[r];
+                e[j] = r + 1 < nruns ? runstart[r + 1] : (int32_t)n;
+                k[j] = runk[r];
             }
+#pragma unroll
+            for (int j = 0; j < U; ++j) one(r0 + j * S, s[j], e[j], k[j]);
+        }
+        for (; r0 < nruns; r0 += S)
+            one(r0, runstart[r0], r0 + 1 < nruns ? runstart[r0 + 1] : (int32_t)n, runk[r0]);
+    }
+    t.sync();
+    // runs of 33..RSUM_CHUNK edges: a warp each.  Longer runs (a cluster's
+    // self-loop run can hold a large part of the graph): their chunks of
+    // RSUM_CHUNK edges are shared out over every warp of the team, then a warp
+    // per run sums its chunk sums -- the same sum as rsum_warp.
+    const int32_t nl = uread(&fl[1]);
+    int64_t nchunks = 0;
+    int32_t *coff = nullptr;
+    double *chunk_sum = nullptr;
+    if (nl > 0) {
+        coff = sc.arena.take<int32_t>((int64_t)nl + 1);
+        if (!sc.arena.ok()) return out;
+        nchunks = team_scan<Team, int64_t>(
+            t, sc, sm, nl,
+            [&](int64_t q) -> int64_t {
+                const int64_t len = longq[q].y - longq[q].x;
+                return len > RSUM_CHUNK ? (len + RSUM_CHUNK - 1) / RSUM_CHUNK : 0;
+            },
+            [&](int64_t q, int64_t pre, int64_t) { coff[q] = (int32_t)pre; });
+        chunk_sum = sc.arena.take<double>(nchunks + 1);
+        if (!sc.arena.ok()) return out;
+    }
+    for (int64_t w = team_warp(t); w < nl + nchunks; w += team_nwarps(t)) {
+        if (w < nl) {
+            const int4 L = longq[w];
+            if (L.y - L.x <= RSUM_CHUNK) {
+                const float v = (float)rsum_chunk_warp(L.y - L.x, [&](int64_t x) { return cost_sorted[L.x + x]; });
+                if (lane_id() == 0) finish(L.z, v);
+            }
+        } else {
+            // chunk g belongs to the last run q with coff[q] <= g
+            const int64_t g = w - nl;
+            int32_t lo = 0, hi = nl - 1;
+            while (lo < hi) {
+                const int32_t mid = (lo + hi + 1) >> 1;
+                if (coff[mid] <= g)
+                    lo = mid;
+                else
+                    hi = mid - 1;
+            }
+            const int4 L = longq[lo];
+            const int64_t base = L.x + (g - coff[lo]) * RSUM_CHUNK;
+            const int64_t len = L.y - base < RSUM_CHUNK ? L.y - base : RSUM_CHUNK;
+            const double d = rsum_chunk_warp(len, [&](int64_t x) { return cost_sorted[base + x]; });
+            if (lane_id() == 0) chunk_sum[g] = d;
         }
     }
     t.sync();
+    if (nchunks > 0) {
+        for (int64_t w = team_warp(t); w < nl; w += team_nwarps(t)) {
+            const int4 L = longq[w];
+            const int64_t len = L.y - L.x;
+            if (len <= RSUM_CHUNK) continue;
+            const int64_t c0 = coff[w], nc = (len + RSUM_CHUNK - 1) / RSUM_CHUNK;
+            double acc = 0.0;  // lane l: chunks l, l + 32, ... in order
+            for (int64_t c = lane_id(); c < nc; c += 32) acc = __dadd_rn(acc, chunk_sum[c0 + c]);
+            const float v = (float)rsum_lane_tree(acc);
+            if (lane_id() == 0) finish(L.z, v);
+        }
+        t.sync();
+    }
     prof_mark(t, sc, PH_CONTRACT_RUNS);
     *bad = uread(&fl[0]);
     // 4. dims and the smallest cost (every new edge has row < col)

@@ -227,19 +227,37 @@ __device__ int32_t matching_contraction_map(const Team &t, Scratch &sc, char *sm
             for (int64_t k = t.rank(); k < ntouch_prev; k += t.size()) next_offer[Tp[k]] = 0ull;
             // (the pairs are counted at their smaller end, one atomic per warp)
             int32_t mine = 0;
-            for (int64_t kb = t.rank() - lane_id(); kb < ntouch; kb += t.size()) {
-                const int64_t k = kb + lane_id();
-                if (k < ntouch) {
-                    const int32_t v = T0[k];
-                    const unsigned long long o = cur_offer[v];
-                    const int32_t b = (int32_t)(~(uint32_t)(o & 0xffffffffull));
-                    const unsigned long long ob = cur_offer[b];
-                    if (ob && (int32_t)(~(uint32_t)(ob & 0xffffffffull)) == v && v < b) {
-                        nm[b] = v;
-                        matched[v] = 1;
-                        matched[b] = 1;
-                        ++mine;
-                    }
+            auto offered = [](unsigned long long o) { return (int32_t)(~(uint32_t)(o & 0xffffffffull)); };
+            auto pair_up = [&](int32_t v, int32_t b, unsigned long long ob) {
+                if (ob && offered(ob) == v && v < b) {
+                    nm[b] = v;
+                    matched[v] = 1;
+                    matched[b] = 1;
+                    ++mine;
+                }
+            };
+            {
+                // four touched vertices a thread at a time: their chains of
+                // loads (vertex, its offer, the partner's offer) overlap
+                constexpr int U = 4;
+                const int64_t S = t.size();
+                int64_t k0 = t.rank();
+                for (; k0 + (U - 1) * S < ntouch; k0 += U * S) {
+                    int32_t v[U], b[U];
+                    unsigned long long ob[U];
+#pragma unroll
+                    for (int k = 0; k < U; ++k) v[k] = T0[k0 + k * S];
+#pragma unroll
+                    for (int k = 0; k < U; ++k) b[k] = offered(cur_offer[v[k]]);
+#pragma unroll
+                    for (int k = 0; k < U; ++k) ob[k] = cur_offer[b[k]];
+#pragma unroll
+                    for (int k = 0; k < U; ++k) pair_up(v[k], b[k], ob[k]);
+                }
+                for (; k0 < ntouch; k0 += S) {
+                    const int32_t v = T0[k0];
+                    const int32_t b = offered(cur_offer[v]);
+                    pair_up(v, b, cur_offer[b]);
                 }
             }
             mine = warp_sum(mine);
@@ -251,6 +269,7 @@ __device__ int32_t matching_contraction_map(const Team &t, Scratch &sc, char *sm
             float rel = (float)(curm - prev) / ((float)prev + 1.0f);
             prev = curm;
             ntouch_prev = ntouch;
+            if (it == 0) prof_mark(t, sc, PH_MATCH_FIRST);
             if (pairs == 0 || (double)rel < 0.1) break;
             // vertices matched in this iteration take no offers in the next:
             // the next offer pass reads `matched` after this sync
@@ -266,8 +285,10 @@ __device__ int32_t matching_contraction_map(const Team &t, Scratch &sc, char *sm
     team_scan<Team, int64_t>(
         t, sc, sm, M, [&](int64_t v) -> int64_t { return nm[v] == (int32_t)v ? 1 : 0; },
         [&](int64_t v, int64_t pre, int64_t) { rank[v] = (int32_t)pre; });
-    for (int64_t v = t.rank(); v < M; v += t.size()) map_out[v] = rank[nm[v]];
+    team_for_batched(
+        t, M, [&](int64_t v) { return rank[nm[v]]; }, [&](int64_t v, int32_t r) { map_out[v] = r; });
     t.sync();
+    prof_mark(t, sc, PH_MATCH_LABELS);
     sc.arena.release(mark);
     return prev;
 }

@@ -44,6 +44,43 @@ __device__ __forceinline__ int64_t find_edge(const int32_t *off, const int32_t *
     return (lo < off[a + 1] && col[lo] == b) ? lo : -1;
 }
 
+// find_edge of three (a, b) pairs at once: the three binary searches step in
+// lockstep, so each step's loads are in flight together
+__device__ __forceinline__ void find_edges3(const int32_t *off, const int32_t *col, const int32_t (&a)[3],
+                                           const int32_t (&b)[3], int32_t (&out)[3])
+{
+    int32_t lo[3], hi[3], end[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        lo[k] = off[a[k]];
+        hi[k] = end[k] = off[a[k] + 1];
+    }
+    for (int step = 0; step < 32; ++step) {
+        int32_t m[3], c[3];
+        bool any = false;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            m[k] = (lo[k] + hi[k]) >> 1;
+            c[k] = lo[k] < hi[k] ? col[m[k]] : 0;
+        }
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+            if (lo[k] < hi[k]) {
+                any = true;
+                if (c[k] < b[k])
+                    lo[k] = m[k] + 1;
+                else
+                    hi[k] = m[k];
+            }
+        if (!any) break;
+    }
+    int32_t c[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) c[k] = lo[k] < end[k] ? col[lo[k]] : 0;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) out[k] = (lo[k] < end[k] && c[k] == b[k]) ? lo[k] : -1;
+}
+
 // number of entries of row a with col < b, plus all rows < a
 __device__ __forceinline__ int64_t lower_edge(const int32_t *off, const int32_t *col, int32_t a, int32_t b)
 {
@@ -65,6 +102,7 @@ __device__ bool mp_build(const Team &t, Scratch &sc, char *sm, const Graph &A, T
     int32_t nmax = A.max_dim();
     // normalize_triangles (:79)
     const int64_t T = tri_normalize(t, sc, sm, tb.t1, tb.t2, tb.t3, tb.num, nmax);
+    prof_mark(t, sc, PH_MP_NORM);
     if (!sc.arena.ok()) return false;
     mp.T = T;
     mp.t1 = tb.t1;
@@ -77,16 +115,21 @@ __device__ bool mp_build(const Team &t, Scratch &sc, char *sm, const Graph &A, T
     if (!sc.arena.ok()) return false;
     team_offsets(t, A.n, nmax, [&](int64_t e) { return A.row[e]; }, aoff);
     const int nb = bits_for((uint64_t)(nmax > 0 ? nmax : 1));
-    // chords not in A
+    // chords not in A: the three sides of each triangle are looked up
+    // together, and the compaction reads the flags (nv2 is free until the
+    // chord sort)
+    uint8_t *absent = reinterpret_cast<uint8_t *>(nv2);
+    for (int64_t k = t.rank(); k < T; k += t.size()) {
+        const int32_t a[3] = {mp.t1[k], mp.t1[k], mp.t2[k]};
+        const int32_t b[3] = {mp.t2[k], mp.t3[k], mp.t3[k]};
+        int32_t f[3];
+        find_edges3(aoff, A.col, a, b, f);
+#pragma unroll
+        for (int s = 0; s < 3; ++s) absent[3 * k + s] = f[s] < 0;
+    }
+    t.sync();
     const int64_t nn = team_compact(
-        t, sc, sm, 3 * T,
-        [&](int64_t q) {
-            int64_t k = q / 3;
-            int s = (int)(q % 3);
-            int32_t a = s == 2 ? mp.t2[k] : mp.t1[k];
-            int32_t b = s == 0 ? mp.t2[k] : mp.t3[k];
-            return find_edge(aoff, A.col, a, b) < 0;
-        },
+        t, sc, sm, 3 * T, [&](int64_t q) { return absent[q] != 0; },
         [&](int64_t q, int64_t p) {
             int64_t k = q / 3;
             int s = (int)(q % 3);
@@ -164,6 +207,7 @@ __device__ bool mp_build(const Team &t, Scratch &sc, char *sm, const Graph &A, T
         mp.cost[p] = 0.0f;
     }
     t.sync();
+    prof_mark(t, sc, PH_MP_CHORDS);
     // merged row offsets, correspondences (compute_triangle_edge_correspondence, :15-62)
     int32_t *moff = aoff;  // reuse
     team_offsets(t, E, nmax, [&](int64_t e) { return mp.row[e]; }, moff);
@@ -181,10 +225,11 @@ __device__ bool mp_build(const Team &t, Scratch &sc, char *sm, const Graph &A, T
     int32_t *w1 = sc.arena.take<int32_t>(3 * T + 1), *w2 = sc.arena.take<int32_t>(3 * T + 1);
     if (!sc.arena.ok()) return false;
     for (int64_t k = t.rank(); k < T; k += t.size()) {
-        int32_t a = mp.t1[k], b = mp.t2[k], c = mp.t3[k];
-        int32_t x = (int32_t)find_edge(moff, mp.col, a, b);
-        int32_t y = (int32_t)find_edge(moff, mp.col, a, c);
-        int32_t z = (int32_t)find_edge(moff, mp.col, b, c);
+        const int32_t a = mp.t1[k], b = mp.t2[k], c = mp.t3[k];
+        const int32_t from[3] = {a, a, b}, to[3] = {b, c, c};
+        int32_t f[3];
+        find_edges3(moff, mp.col, from, to, f);
+        const int32_t x = f[0], y = f[1], z = f[2];
         mp.e12[k] = x;
         mp.e13[k] = y;
         mp.e23[k] = z;
@@ -213,6 +258,7 @@ __device__ bool mp_build(const Team &t, Scratch &sc, char *sm, const Graph &A, T
         team_offsets(t, 3 * T, (int32_t)E, [&](int64_t k) { return (int32_t)qk[k]; }, mp.inc_off);
     }
     sc.arena.release(ik);
+    prof_mark(t, sc, PH_MP_INCID);
     // each covered edge's share of its cost, and the edges whose incoming
     // messages a whole warp sums
     mp.share = sc.arena.take<float>(E + 1);
@@ -279,10 +325,9 @@ template <class Team>
 __device__ void mp_iteration(const Team &t, const Mp &mp)
 {
     const double third = 1.0 / 3.0, half = 1.0 / 2.0;
-    for (int64_t k = t.rank(); k < mp.T; k += t.size()) {
-        float t12 = __fadd_rn(mp.c12[k], mp.share[mp.e12[k]]);
-        float t13 = __fadd_rn(mp.c13[k], mp.share[mp.e13[k]]);
-        float t23 = __fadd_rn(mp.c23[k], mp.share[mp.e23[k]]);
+    // the six moves of one triangle, from its three costs (the edges' shares
+    // added); writes the triangle's costs and its messages to the edges
+    auto moves = [&](int64_t k, float t12, float t13, float t23) {
         float e12 = 0.0f, e13 = 0.0f, e23 = 0.0f;
         {
             float mm = min_marginal(t12, t13, t23);
@@ -320,15 +365,60 @@ __device__ void mp_iteration(const Team &t, const Mp &mp)
         mp.slot[mp.pos[3 * k]] = e12;
         mp.slot[mp.pos[3 * k + 1]] = e13;
         mp.slot[mp.pos[3 * k + 2]] = e23;
+    };
+    {
+        // two triangles a thread at a time: their loads and the gathers of
+        // the edges' shares are in flight together
+        const int64_t S = t.size();
+        int64_t k = t.rank();
+        for (; k + S < mp.T; k += 2 * S) {
+            const int64_t k2 = k + S;
+            const int32_t a12 = mp.e12[k], a13 = mp.e13[k], a23 = mp.e23[k];
+            const int32_t b12 = mp.e12[k2], b13 = mp.e13[k2], b23 = mp.e23[k2];
+            const float ac12 = mp.c12[k], ac13 = mp.c13[k], ac23 = mp.c23[k];
+            const float bc12 = mp.c12[k2], bc13 = mp.c13[k2], bc23 = mp.c23[k2];
+            const float as12 = mp.share[a12], as13 = mp.share[a13], as23 = mp.share[a23];
+            const float bs12 = mp.share[b12], bs13 = mp.share[b13], bs23 = mp.share[b23];
+            moves(k, __fadd_rn(ac12, as12), __fadd_rn(ac13, as13), __fadd_rn(ac23, as23));
+            moves(k2, __fadd_rn(bc12, bs12), __fadd_rn(bc13, bs13), __fadd_rn(bc23, bs23));
+        }
+        for (; k < mp.T; k += S)
+            moves(k, __fadd_rn(mp.c12[k], mp.share[mp.e12[k]]), __fadd_rn(mp.c13[k], mp.share[mp.e13[k]]),
+                  __fadd_rn(mp.c23[k], mp.share[mp.e23[k]]));
     }
     t.sync();
     // covered edges: c = 0 + RSUM(messages); long runs by a warp
-    for (int64_t e = t.rank(); e < mp.E; e += t.size()) {
-        const int32_t s = mp.inc_off[e], n = mp.inc_off[e + 1] - s;
-        if (n == 0 || n > RSUM_THREAD_MAX) continue;
-        const float c = __fadd_rn(0.0f, rsum_upto8(mp.slot + s, n));
-        mp.cost[e] = c;
-        mp.share[e] = __fdiv_rn(c, (float)n);
+    {
+        // four edges a thread at a time: offsets, then the messages, then
+        // the stores
+        constexpr int U = 4;
+        const int64_t S = t.size();
+        int64_t e0 = t.rank();
+        for (; e0 + (U - 1) * S < mp.E; e0 += U * S) {
+            int32_t s[U], n[U];
+            float c[U];
+#pragma unroll
+            for (int k = 0; k < U; ++k) {
+                s[k] = mp.inc_off[e0 + k * S];
+                n[k] = mp.inc_off[e0 + k * S + 1] - s[k];
+            }
+#pragma unroll
+            for (int k = 0; k < U; ++k)
+                c[k] = (n[k] == 0 || n[k] > RSUM_THREAD_MAX) ? 0.0f : __fadd_rn(0.0f, rsum_upto8(mp.slot + s[k], n[k]));
+#pragma unroll
+            for (int k = 0; k < U; ++k)
+                if (n[k] != 0 && n[k] <= RSUM_THREAD_MAX) {
+                    mp.cost[e0 + k * S] = c[k];
+                    mp.share[e0 + k * S] = __fdiv_rn(c[k], (float)n[k]);
+                }
+        }
+        for (; e0 < mp.E; e0 += S) {
+            const int32_t s = mp.inc_off[e0], n = mp.inc_off[e0 + 1] - s;
+            if (n == 0 || n > RSUM_THREAD_MAX) continue;
+            const float c = __fadd_rn(0.0f, rsum_upto8(mp.slot + s, n));
+            mp.cost[e0] = c;
+            mp.share[e0] = __fdiv_rn(c, (float)n);
+        }
     }
     for (int64_t q = team_warp(t); q < mp.nlong; q += team_nwarps(t)) {
         const int32_t e = mp.longe[q];
@@ -353,7 +443,7 @@ __device__ double dual_update_cycle_length(const Team &t, Scratch &sc, char *sm,
     TriBuf tb;
     prof_mark(t, sc, PH_OTHER);
     conflicted_cycles(t, sc, sm, A, c, tri_factor, tol, tb);
-    prof_mark(t, sc, PH_CYCLES);
+    prof_mark(t, sc, PH_CYC_SEARCH);
     *failed = !sc.arena.ok();
     if (*failed) {
         sc.arena.release(m);

@@ -84,7 +84,18 @@ enum Phase : int {
     PH_CSORT_SCATTER = 13,  // ... bucket starts and the scatter
     PH_CSORT_RANK = 14,   // ... ordering within the buckets
     PH_CONTRACT_RUNS = 15,  // contraction: run heads, sums, the new edges
-    PH_COUNT = 16
+    PH_MATCH_LABELS = 16,   // matching: labels of the contraction map
+    PH_MATCH_FIRST = 17,    // matching: the first offer / match iteration (reads every edge)
+    PH_WOC_MSF = 18,        // forest: attractive edges and their maximum spanning forest
+    PH_WOC_CSR = 19,        // forest: the forest's symmetric lists
+    PH_WOC_CHECKS = 20,     // forest: components, cycle checks, thresholds
+    PH_WOC_ROOT = 21,       // forest: rooting (level-synchronous BFS)
+    PH_WOC_PATHS = 22,      // forest: path lengths and bottleneck cuts
+    PH_CYC_SEARCH = 23,     // cycle search: the expansions after the CSR
+    PH_MP_NORM = 24,        // message passing: triangle normalisation
+    PH_MP_CHORDS = 25,      // message passing: chords and the merged edge list
+    PH_MP_INCID = 26,       // message passing: triangle-edge correspondence, incidence order
+    PH_COUNT = 27
 };
 
 __device__ __forceinline__ uint64_t prof_now()
@@ -222,11 +233,55 @@ __device__ __forceinline__ T warp_fold_parts(const T *part, int nb, T init, Op o
     return r;
 }
 
+// Grid-stride loop over [0, n) in batches of U strides: load(i) for every
+// item of a batch first (loads only), then store(i, value) for each, so a
+// batch waits for one memory round trip instead of U.  Per thread the items
+// keep their order; a load must not read what the store of an earlier item
+// of the same thread writes.
+template <int U = 4, class Team, class Load, class Store>
+__device__ __forceinline__ void team_for_batched(const Team &t, int64_t n, Load load, Store store)
+{
+    const int64_t S = t.size();
+    int64_t i0 = t.rank();
+    for (; i0 + (U - 1) * S < n; i0 += S * U) {
+        decltype(load(int64_t(0))) v[U];
+#pragma unroll
+        for (int k = 0; k < U; ++k) v[k] = load(i0 + k * S);
+#pragma unroll
+        for (int k = 0; k < U; ++k) store(i0 + k * S, v[k]);
+    }
+    for (; i0 < n; i0 += S) store(i0, load(i0));
+}
+
+// the sum over the team of one value per thread; one team sync
+template <class Team, class T>
+__device__ T team_total(const Team &t, Scratch &sc, char *sm, T v)
+{
+    const T s = block_sum<T>(v, reinterpret_cast<T *>(sm));
+    T *part = reinterpret_cast<T *>(sc.next_part());
+    if (threadIdx.x == 0) part[t.block()] = s;
+    t.sync();
+    return warp_fold_parts<T>(part, t.nblocks(), T(0), [](T a, T b) { return a + b; });
+}
+
 template <class Team, class T, class Get>
 __device__ T team_sum(const Team &t, Scratch &sc, char *sm, int64_t n, Get get)
 {
     T s = T(0);
-    for (int64_t i = t.rank(); i < n; i += t.size()) s += get(i);
+    {
+        // four strides at a time, loads issued together
+        constexpr int U = 4;
+        const int64_t S = t.size();
+        int64_t i = t.rank();
+        for (; i + (U - 1) * S < n; i += U * S) {
+            T v[U];
+#pragma unroll
+            for (int k = 0; k < U; ++k) v[k] = get(i + k * S);
+#pragma unroll
+            for (int k = 0; k < U; ++k) s += v[k];
+        }
+        for (; i < n; i += S) s += get(i);
+    }
     s = block_sum<T>(s, reinterpret_cast<T *>(sm));
     T *part = reinterpret_cast<T *>(sc.next_part());
     if (threadIdx.x == 0) part[t.block()] = s;
@@ -238,9 +293,21 @@ template <class Team, class T, class Get>
 __device__ T team_max(const Team &t, Scratch &sc, char *sm, int64_t n, T init, Get get)
 {
     T s = init;
-    for (int64_t i = t.rank(); i < n; i += t.size()) {
-        T x = get(i);
-        s = x > s ? x : s;
+    {
+        constexpr int U = 4;
+        const int64_t S = t.size();
+        int64_t i = t.rank();
+        for (; i + (U - 1) * S < n; i += U * S) {
+            T x[U];
+#pragma unroll
+            for (int k = 0; k < U; ++k) x[k] = get(i + k * S);
+#pragma unroll
+            for (int k = 0; k < U; ++k) s = x[k] > s ? x[k] : s;
+        }
+        for (; i < n; i += S) {
+            T x = get(i);
+            s = x > s ? x : s;
+        }
     }
     s = block_max<T>(s, reinterpret_cast<T *>(sm));
     T *part = reinterpret_cast<T *>(sc.next_part());
@@ -272,11 +339,30 @@ __device__ void team_maxi_minf(const Team &t, Scratch &sc, char *sm, int64_t n, 
 {
     int32_t a = iinit;
     float b = finit;
-    for (int64_t i = t.rank(); i < n; i += t.size()) {
-        const int32_t x = ia(i);
-        const float y = fb(i);
-        a = x > a ? x : a;
-        b = y < b ? y : b;
+    {
+        constexpr int U = 4;
+        const int64_t S = t.size();
+        int64_t i = t.rank();
+        for (; i + (U - 1) * S < n; i += U * S) {
+            int32_t x[U];
+            float y[U];
+#pragma unroll
+            for (int k = 0; k < U; ++k) {
+                x[k] = ia(i + k * S);
+                y[k] = fb(i + k * S);
+            }
+#pragma unroll
+            for (int k = 0; k < U; ++k) {
+                a = x[k] > a ? x[k] : a;
+                b = y[k] < b ? y[k] : b;
+            }
+        }
+        for (; i < n; i += S) {
+            const int32_t x = ia(i);
+            const float y = fb(i);
+            a = x > a ? x : a;
+            b = y < b ? y : b;
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
@@ -347,7 +433,20 @@ __device__ T team_scan(const Team &t, Scratch &sc, char *sm, int64_t n, In in, O
     int64_t lo, hi;
     block_chunk(t, n, lo, hi);
     T s = T(0);
-    for (int64_t i = lo + threadIdx.x; i < hi; i += blockDim.x) s += in(i);
+    {
+        // four strides at a time, loads issued together
+        constexpr int U = 4;
+        const int64_t S = blockDim.x;
+        int64_t i = lo + threadIdx.x;
+        for (; i + (U - 1) * S < hi; i += U * S) {
+            T v[U];
+#pragma unroll
+            for (int k = 0; k < U; ++k) v[k] = in(i + k * S);
+#pragma unroll
+            for (int k = 0; k < U; ++k) s += v[k];
+        }
+        for (; i < hi; i += S) s += in(i);
+    }
     s = block_sum<T>(s, tsm);
     T *part = reinterpret_cast<T *>(sc.next_part());
     if (threadIdx.x == 0) part[t.block()] = s;
@@ -472,7 +571,19 @@ __device__ double team_csum_count(const Team &t, Scratch &sc, int64_t n, Get get
     if (sc.arena.ok() && t.block() == 0 && warp_in_block() == 0) {
         csum_t a = {0.0, 0.0};
         int64_t c = 0;
-        for (int64_t k = lane_id(); k < nch; k += 32) {
+        // a lane merges partials k, k + 32, ... in order, eight loaded at a time
+        int64_t k = lane_id();
+        for (; k + 7 * 32 < nch; k += 8 * 32) {
+            csum_t x[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                x[j] = parts[k + 32 * j];
+                c += pcnt[k + 32 * j];
+            }
+#pragma unroll
+            for (int j = 0; j < 8; ++j) a = cs_merge(a, x[j]);
+        }
+        for (; k < nch; k += 32) {
             a = cs_merge(a, parts[k]);
             c += pcnt[k];
         }
@@ -546,18 +657,73 @@ __device__ __forceinline__ float rsum_upto8(const float *p, int n)
     return (float)__dadd_rn(a, b);
 }
 
-// the same sum by a whole warp (any n); result valid on every lane
-template <class Get>
-__device__ __forceinline__ float rsum_warp(int64_t n, Get v)
+// The same sum by one thread for n <= 32 values at p[0, n): the complete
+// tree over 32 lanes (+0.0 in the empty ones) is the pairwise sum of four
+// complete trees over 8 (each as in rsum_upto8), so this equals
+// rsum_serial(n, p[k]); the loads of a group of 8 are issued together.
+__device__ __forceinline__ float rsum_upto32(const float *p, int n)
 {
-    double a = 0.0;
-    for (int64_t k = lane_id(); k < n; k += 32) a = __dadd_rn(a, (double)v(k));
+    double g[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        double x[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) x[k] = 8 * q + k < n ? __dadd_rn(0.0, (double)p[8 * q + k]) : 0.0;
+        g[q] = __dadd_rn(__dadd_rn(__dadd_rn(x[0], x[1]), __dadd_rn(x[2], x[3])),
+                         __dadd_rn(__dadd_rn(x[4], x[5]), __dadd_rn(x[6], x[7])));
+    }
+    return (float)__dadd_rn(__dadd_rn(g[0], g[1]), __dadd_rn(g[2], g[3]));
+}
+
+// Sums of more than RSUM_CHUNK values are defined by chunks: each chunk of
+// RSUM_CHUNK consecutive values is summed as above (kept in double), and the
+// chunk sums are summed the same way (chunk c to lane c mod 32), so that many
+// warps can share one long sum.
+constexpr int64_t RSUM_CHUNK = 4096;
+
+// the pairwise tree over a warp's 32 lane values; the result on every lane
+__device__ __forceinline__ double rsum_lane_tree(double a)
+{
 #pragma unroll
     for (int off = 1; off < 32; off <<= 1) {
         double o = __shfl_down_sync(FULL, a, off);
         if ((lane_id() & (2 * off - 1)) == 0) a = __dadd_rn(a, o);
     }
-    return (float)__shfl_sync(FULL, a, 0);
+    return __shfl_sync(FULL, a, 0);
+}
+
+// the RSUM of at most RSUM_CHUNK values v(0..len) by a warp, in double (not
+// rounded); a lane adds its values k, k + 32, ... in that order, eight of them
+// loaded at a time
+template <class Get>
+__device__ __forceinline__ double rsum_chunk_warp(int64_t len, Get v)
+{
+    double a = 0.0;
+    int64_t k = lane_id();
+    for (; k + 7 * 32 < len; k += 8 * 32) {
+        float x[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) x[j] = v(k + 32 * j);
+#pragma unroll
+        for (int j = 0; j < 8; ++j) a = __dadd_rn(a, (double)x[j]);
+    }
+    for (; k < len; k += 32) a = __dadd_rn(a, (double)v(k));
+    return rsum_lane_tree(a);
+}
+
+// the same sum by a whole warp (any n); result valid on every lane
+template <class Get>
+__device__ __forceinline__ float rsum_warp(int64_t n, Get v)
+{
+    if (n <= RSUM_CHUNK) return (float)rsum_chunk_warp(n, v);
+    double acc = 0.0;  // this lane's chunks: c = lane, lane + 32, ...
+    for (int64_t c = 0; c * RSUM_CHUNK < n; ++c) {
+        const int64_t base = c * RSUM_CHUNK;
+        const int64_t len = n - base < RSUM_CHUNK ? n - base : RSUM_CHUNK;
+        const double d = rsum_chunk_warp(len, [&](int64_t k) { return v(base + k); });
+        if (lane_id() == (int)(c & 31)) acc = __dadd_rn(acc, d);
+    }
+    return (float)rsum_lane_tree(acc);
 }
 
 // ---------------------------------------------------------------------------
@@ -921,12 +1087,23 @@ __device__ __forceinline__ void smem_bitonic(uint64_t *key, int32_t *idx, int m,
 struct NoBigKey {
     __device__ uint64_t operator()(int64_t) const { return 0; }
 };
+struct NoNote {
+    __device__ void operator()(int64_t, int64_t) const {}
+};
 
-template <class Team, class BkSlot, class Bk, class Sub, class Pay, class BigKey = NoBigKey>
+// Items handled at once by a thread in the sort's streaming passes: their
+// loads are issued together, so a pass waits for one memory round trip per
+// batch instead of one per item.
+constexpr int SORT_BATCH = 4;
+
+// bk_slot(i) must only load: its value carries the bucket in the low 32 bits
+// (the high 32 bits are the caller's), and note(i, value) stores whatever the
+// caller keeps of it once the batch's loads are done.
+template <class Team, class BkSlot, class Bk, class Sub, class Pay, class BigKey = NoBigKey, class Note = NoNote>
 __device__ bool team_bucket_sort_ex(const Team &t, Scratch &sc, char *sm, int64_t n, int32_t nb, BkSlot bk_slot,
                                     Bk bucket, Sub sub, Pay pay, uint64_t *keys_out, int32_t *idx_out,
                                     int32_t *bstart, int32_t *bucket_out = nullptr, int detail_phase = -1,
-                                    BigKey big_key = BigKey(), int big_bits = 0)
+                                    BigKey big_key = BigKey(), int big_bits = 0, Note note = Note())
 {
     uint64_t am = sc.arena.mark();
     int32_t *slot = sc.arena.take<int32_t>(n + 1);
@@ -940,17 +1117,39 @@ __device__ bool team_bucket_sort_ex(const Team &t, Scratch &sc, char *sm, int64_
     for (int64_t b = t.rank(); b <= nb; b += t.size()) bstart[b] = 0;
     if (t.rank() < 4) nlist[t.rank()] = 0;
     t.sync();
-    // slots: the lanes of a warp that share a bucket take theirs with one atomic
-    for (int64_t base = (int64_t)t.rank() - lane_id(); base < n; base += t.size()) {
-        const int64_t i = base + lane_id();
-        const bool valid = i < n;
-        const int32_t b = valid ? (int32_t)bk_slot(i) : -1;
-        const unsigned peers = __match_any_sync(FULL, b);
-        const int leader = __ffs(peers) - 1;
-        int32_t s0 = 0;
-        if (valid && lane_id() == leader) s0 = atomicAdd(&bstart[b], __popc(peers));
-        s0 = __shfl_sync(FULL, s0, leader);
-        if (valid) slot[i] = s0 + __popc(peers & lanemask_lt());
+    // slots: the lanes of a warp that share a bucket take theirs with one
+    // atomic; a warp handles SORT_BATCH strides at once (item k of a batch is
+    // base + k * size + lane)
+    {
+        constexpr int U = SORT_BATCH;
+        const int64_t S = t.size();
+        for (int64_t base = (int64_t)t.rank() - lane_id(); base < n; base += S * U) {
+            int64_t w[U];
+#pragma unroll
+            for (int k = 0; k < U; ++k) {
+                const int64_t i = base + k * S + lane_id();
+                w[k] = i < n ? (int64_t)bk_slot(i) : int64_t(-1);
+            }
+            int32_t s0[U];
+            unsigned peers[U];
+#pragma unroll
+            for (int k = 0; k < U; ++k) {
+                const int64_t i = base + k * S + lane_id();
+                const int32_t b = i < n ? (int32_t)(uint32_t)w[k] : -1;
+                peers[k] = __match_any_sync(FULL, b);
+                s0[k] = 0;
+                if (i < n && lane_id() == __ffs(peers[k]) - 1) s0[k] = atomicAdd(&bstart[b], __popc(peers[k]));
+            }
+#pragma unroll
+            for (int k = 0; k < U; ++k) {
+                const int64_t i = base + k * S + lane_id();
+                const int32_t s = __shfl_sync(FULL, s0[k], __ffs(peers[k]) - 1);
+                if (i < n) {
+                    slot[i] = s + __popc(peers[k] & lanemask_lt());
+                    note(i, w[k]);
+                }
+            }
+        }
     }
     t.sync();
     if (detail_phase >= 0) prof_mark(t, sc, detail_phase);
@@ -974,36 +1173,92 @@ __device__ bool team_bucket_sort_ex(const Team &t, Scratch &sc, char *sm, int64_
     }
     if (t.rank() == 0) bstart[nb] = (int32_t)n;
     t.sync();
-    for (int64_t i = t.rank(); i < n; i += t.size()) {
-        const int32_t b = (int32_t)bucket(i);
-        const int64_t p = (int64_t)bstart[b] + slot[i];
-        tk[p] = sub(i);
-        ti[p] = pay(i);
-        tb[p] = b;
+    {
+        // full batches of SORT_BATCH strides (loads first, then the
+        // gathers of the bucket starts, then the stores), then one at a time
+        constexpr int U = SORT_BATCH;
+        const int64_t S = t.size();
+        int64_t i0 = t.rank();
+        for (; i0 + (U - 1) * S < n; i0 += U * S) {
+            int32_t b[U], p[U], pv[U];
+            uint64_t kv[U];
+#pragma unroll
+            for (int k = 0; k < U; ++k) {
+                b[k] = (int32_t)bucket(i0 + k * S);
+                p[k] = slot[i0 + k * S];
+                kv[k] = sub(i0 + k * S);
+                pv[k] = pay(i0 + k * S);
+            }
+#pragma unroll
+            for (int k = 0; k < U; ++k) p[k] += bstart[b[k]];
+#pragma unroll
+            for (int k = 0; k < U; ++k) {
+                tk[p[k]] = kv[k];
+                ti[p[k]] = pv[k];
+                tb[p[k]] = b[k];
+            }
+        }
+        for (; i0 < n; i0 += S) {
+            const int32_t b = (int32_t)bucket(i0);
+            const int64_t p = (int64_t)bstart[b] + slot[i0];
+            tk[p] = sub(i0);
+            ti[p] = pay(i0);
+            tb[p] = b;
+        }
     }
     t.sync();
     if (detail_phase >= 0) prof_mark(t, sc, detail_phase + 1);
     // up to 64 items: each item's rank in its bucket is the number of smaller
     // keys there (neighbouring threads read the same bucket)
-    for (int64_t p = t.rank(); p < n; p += t.size()) {
-        const int32_t b = tb[p], s = bstart[b], e = bstart[b + 1];
-        if (e - s > 64) {
-            if (e - s <= BUCKET_MAX) {
-                keys_out[p] = tk[p];
-                idx_out[p] = ti[p];
-                if (bucket_out) bucket_out[p] = b;
+    {
+        // the rank of item p in its bucket; -1: sorted below (a bucket of
+        // 65..BUCKET_MAX items is copied as it is) or by the big path
+        auto rank_in_bucket = [&](int64_t p, int32_t s, int32_t e, uint64_t key) -> int32_t {
+            if (e - s > 64) return e - s <= BUCKET_MAX ? (int32_t)p : -1;
+            int32_t r = 0;
+            for (int32_t q = s; q < e; ++q) {
+                const uint64_t o = tk[q];
+                r += o < key || (o == key && q < p);
             }
-            continue;
+            return s + r;
+        };
+        constexpr int U = SORT_BATCH;
+        const int64_t S = t.size();
+        int64_t p0 = t.rank();
+        for (; p0 + (U - 1) * S < n; p0 += U * S) {
+            int32_t b[U], s[U], e[U], iv[U], dst[U];
+            uint64_t kv[U];
+#pragma unroll
+            for (int k = 0; k < U; ++k) {
+                b[k] = tb[p0 + k * S];
+                kv[k] = tk[p0 + k * S];
+                iv[k] = ti[p0 + k * S];
+            }
+#pragma unroll
+            for (int k = 0; k < U; ++k) {
+                s[k] = bstart[b[k]];
+                e[k] = bstart[b[k] + 1];
+            }
+#pragma unroll
+            for (int k = 0; k < U; ++k) dst[k] = rank_in_bucket(p0 + k * S, s[k], e[k], kv[k]);
+#pragma unroll
+            for (int k = 0; k < U; ++k)
+                if (dst[k] >= 0) {
+                    keys_out[dst[k]] = kv[k];
+                    idx_out[dst[k]] = iv[k];
+                    if (bucket_out) bucket_out[dst[k]] = b[k];
+                }
         }
-        const uint64_t k = tk[p];
-        int32_t r = 0;
-        for (int32_t q = s; q < e; ++q) {
-            const uint64_t o = tk[q];
-            r += o < k || (o == k && q < p);
+        for (; p0 < n; p0 += S) {
+            const int32_t b = tb[p0];
+            const uint64_t key = tk[p0];
+            const int32_t dst = rank_in_bucket(p0, bstart[b], bstart[b + 1], key);
+            if (dst >= 0) {
+                keys_out[dst] = key;
+                idx_out[dst] = ti[p0];
+                if (bucket_out) bucket_out[dst] = b;
+            }
         }
-        keys_out[s + r] = k;
-        idx_out[s + r] = ti[p];
-        if (bucket_out) bucket_out[s + r] = b;
     }
     t.sync();
     // 65..256 items: a warp, bitonic in its share of the staging area

@@ -155,10 +155,13 @@ __device__ void solve_instance(const Team &t, char *sm, Scratch sc, Instance *io
                         break;
                     }
                     // map_node_labels (src/rama_cuda.cu:32-52)
-                    for (int64_t v = t.rank(); v < N0; v += t.size()) {
-                        int32_t m = nm[v];
-                        if (m < msize) nm[v] = map[m];
-                    }
+                    team_for_batched(
+                        t, N0,
+                        [&](int64_t v) {
+                            const int32_t m = nm[v];
+                            return m < msize ? map[m] : m;
+                        },
+                        [&](int64_t v, int32_t m) { nm[v] = m; });
                     t.sync();
                     prof_mark(t, sc, PH_OTHER);
                     ++rounds;

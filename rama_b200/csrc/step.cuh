@@ -43,6 +43,12 @@ __device__ void run_step(const Team &t, char *sm, Scratch sc, rama_step_args *a)
         int32_t mx = team_max<Team, int32_t>(t, sc, sm, a->map_size, 0, [&](int64_t k) { return a->map[k]; });
         Graph g = graph_contract_raw(t, sc, sm, A, a->map, mx);
         if (sc.arena.ok()) copy_graph_out(t, g, a);
+    } else if (op == RAMA_STEP_COARSEN) {
+        int32_t mx = team_max<Team, int32_t>(t, sc, sm, a->map_size, 0, [&](int64_t k) { return a->map[k]; });
+        int bad = 0;
+        Graph g = graph_contract(t, sc, sm, A, a->map, mx, &bad);
+        if (sc.arena.ok()) copy_graph_out(t, g, a);
+        if (t.leader()) a->out_nr = bad;
     } else if (op == RAMA_STEP_MATCHING) {
         int32_t M = 0;
         int32_t nr = matching_contraction_map(t, sc, sm, A, a->mean_multiplier_mm, a->out_map, &M);

@@ -505,6 +505,7 @@ __device__ int32_t woc_contraction_map(const Team &t, Scratch &sc, char *sm, con
                   [&](int64_t p) { return A.col[pidx[p]]; }, [&](int64_t p) { return A.cost[pidx[p]]; }, chosen)) {
         *err |= ERR_ITER_LIMIT;
     }
+    prof_mark(t, sc, PH_WOC_MSF);
     // 3. forest as a symmetric (row,col)-sorted list + CSR
     uint8_t *ekeep = sc.arena.take<uint8_t>(A.n + 1);
     if (!sc.arena.ok()) return 0;
@@ -537,6 +538,7 @@ __device__ int32_t woc_contraction_map(const Team &t, Scratch &sc, char *sm, con
     for (int64_t k = t.rank(); k < F.m2; k += t.size()) F.inv[k] = 0;
     if (t.rank() < 8) F.cnt[t.rank()] = 0;
     t.sync();
+    prof_mark(t, sc, PH_WOC_CSR);
     if (F.m2 == 0) {
         sc.arena.release(mark);
         return 0;
@@ -552,6 +554,7 @@ __device__ int32_t woc_contraction_map(const Team &t, Scratch &sc, char *sm, con
     }
     // 5. edge_contractions_woc_thrust::find_contraction_mapping (:544-599)
     int64_t R = forest_filter_by_cc(t, sc, sm, F);
+    prof_mark(t, sc, PH_WOC_CHECKS);
     int32_t dr = 0, dc = 0, itr = 0;
     int32_t lmin = -1;           // shortest path length of this epoch (-1: stale)
     int thr_noop_version = -1;   // forest version at which thresholding was a no-op
@@ -568,6 +571,7 @@ __device__ int32_t woc_contraction_map(const Team &t, Scratch &sc, char *sm, con
             } else {
                 thr_noop_version = F.version;
             }
+            prof_mark(t, sc, PH_WOC_CHECKS);
         }
         if (R == 0 || F.m2 == 0) break;
         for (int side = 0; side < 2; ++side) {
@@ -577,13 +581,18 @@ __device__ int32_t woc_contraction_map(const Team &t, Scratch &sc, char *sm, con
                 ++dc;
             if (lmin < 0) {
                 if (!forest_root(t, sc, sm, F)) *err |= ERR_ITER_LIMIT;
+                prof_mark(t, sc, PH_WOC_ROOT);
                 lmin = forest_path_lengths(t, sc, sm, F);
+                prof_mark(t, sc, PH_WOC_PATHS);
             }
             if (dr + dc == lmin) {
-                if (forest_resolve(t, sc, sm, F, dr, dc)) {
+                const bool cut = forest_resolve(t, sc, sm, F, dr, dc);
+                prof_mark(t, sc, PH_WOC_PATHS);
+                if (cut) {
                     R = forest_filter_by_cc(t, sc, sm, F);
                     dr = dc = 0;
                     lmin = -1;
+                    prof_mark(t, sc, PH_WOC_CHECKS);
                 }
             }
             if (side == 0 && (R == 0 || F.m2 == 0)) break;

@@ -162,6 +162,22 @@ class Solver:
         k = a.out_n
         return r[:k].cpu().numpy(), co[:k].cpu().numpy(), w[:k].cpu().numpy(), a.out_rows, a.out_cols
 
+    def step_coarsen(self, row, col, cost, rows, cols, node_map, team=1):
+        """The solver's contraction of a graph by a node map: parallel edges
+        summed, self-loops removed (dims taken before, as the reference does);
+        returns (row, col, cost, rows, cols, bad)."""
+        a = _lib.StepArgs(op=_lib.STEP["COARSEN"], team=team)
+        keep = []
+        self._graph_args(a, row, col, cost, rows, cols, keep)
+        m = _dev(node_map, np.int32)
+        keep.append(m)
+        a.map, a.map_size = _p(m), len(node_map)
+        r, co, w = self._out_graph(a, len(cost), keep)
+        self._run(a)
+        k = a.out_n
+        return (r[:k].cpu().numpy(), co[:k].cpu().numpy(), w[:k].cpu().numpy(), a.out_rows, a.out_cols,
+                bool(a.out_nr))
+
     def _map_step(self, op, row, col, cost, rows, cols, team, mm=0.05, max_cycle_length=0):
         torch = _torch()
         a = _lib.StepArgs(op=_lib.STEP[op], team=team, mean_multiplier_mm=mm, max_cycle_length=max_cycle_length)

@@ -62,6 +62,62 @@ def test_contract(solver, oracle, g, team):
 
 @pytest.mark.parametrize("team", TEAMS)
 @pytest.mark.parametrize("g", GRAPHS, ids=IDS)
+def test_coarsen(solver, oracle, g, team):
+    """The solver's own contraction (self-loops removed, bad contractions
+    flagged) against contract + has_bad_contractions + remove_diagonal."""
+    _, i, j, c = g
+    G, r, co, w, rows, cols = _G(oracle, i, j, c)
+    rng = np.random.default_rng(8)
+    N = max(rows, cols)
+    m = rng.integers(0, max(N // 3, 1), size=N)
+    _, m = np.unique(m, return_inverse=True)
+    m = m.astype(np.int32)
+    H = G.contract(m)
+    bad = H.has_bad_contractions()
+    H.remove_diagonal()
+    hr, hc, hw = H.arrays()
+    gr, gc, gw, grows, gcols, gbad = solver.step_coarsen(r, co, w, rows, cols, m, team=team)
+    assert np.array_equal(gr, hr) and np.array_equal(gc, hc)
+    assert np.array_equal(gw, hw)
+    assert (grows, gcols) == H.dims
+    assert gbad == bad
+
+
+@pytest.mark.parametrize("nodes,edges,groups", [(3000, 30000, 2), (5000, 60000, 3), (20000, 200000, 5)])
+def test_contract_runs_longer_than_a_chunk(solver, oracle, nodes, edges, groups):
+    """A map onto a few nodes makes self-loop and parallel-edge runs of more
+    than 4096 edges.  The plain contraction sums each by one warp, the
+    solver's coarsening shares their chunks out over many warps; both must
+    equal the oracle's chunked RSUM bit for bit (and the self-loop sums decide
+    the bad-contraction flag)."""
+    rng = np.random.default_rng(nodes)
+    i = rng.integers(0, nodes, size=edges).astype(np.int32)
+    j = rng.integers(0, nodes, size=edges).astype(np.int32)
+    keep = i != j
+    i, j = i[keep], j[keep]
+    c = (rng.normal(size=len(i)) * 10.0 ** rng.integers(-3, 3, size=len(i))).astype(np.float32)
+    G, r, co, w, rows, cols = _G(oracle, i, j, c)
+    N = max(rows, cols)
+    m = (np.arange(N) % groups).astype(np.int32)
+    H = G.contract(m)
+    hr, hc, hw = H.arrays()
+    for team in TEAMS:
+        gr, gc, gw, grows, gcols = solver.step_contract(r, co, w, rows, cols, m, team=team)
+        assert np.array_equal(gr, hr) and np.array_equal(gc, hc)
+        assert np.array_equal(gw, hw)
+        assert (grows, gcols) == H.dims
+    bad = H.has_bad_contractions()
+    H.remove_diagonal()
+    hr, hc, hw = H.arrays()
+    for team in TEAMS:
+        gr, gc, gw, grows, gcols, gbad = solver.step_coarsen(r, co, w, rows, cols, m, team=team)
+        assert np.array_equal(gr, hr) and np.array_equal(gc, hc)
+        assert np.array_equal(gw, hw)
+        assert (grows, gcols) == H.dims and gbad == bad
+
+
+@pytest.mark.parametrize("team", TEAMS)
+@pytest.mark.parametrize("g", GRAPHS, ids=IDS)
 def test_matching(solver, oracle, g, team):
     _, i, j, c = g
     G, r, co, w, rows, cols = _G(oracle, i, j, c)

@@ -364,16 +364,36 @@ def test_csum_exact_on_integers(oracle):
     assert oracle.csum(x) == float(np.sum(x.astype(np.float64)))
 
 
+def _lane_tree(vals):
+    """32 lanes (value k to lane k mod 32, in order, from +0.0), then the
+    pairwise tree over the lanes; in double."""
+    lanes = np.zeros(32)
+    for k, v in enumerate(vals):
+        lanes[k % 32] += float(v)
+    off = 1
+    while off < 32:
+        for l in range(0, 32, 2 * off):
+            lanes[l] = lanes[l] + lanes[l + off]
+        off *= 2
+    return lanes[0]
+
+
 def test_rsum_matches_definition(oracle):
     rng = np.random.default_rng(5)
-    for n in (0, 1, 2, 3, 7, 31, 32, 33, 100, 1000):
+    for n in (0, 1, 2, 3, 7, 31, 32, 33, 100, 1000, 4095, 4096):
         x = rng.normal(size=n).astype(np.float32)
-        lanes = np.zeros(32)
-        for k in range(n):
-            lanes[k % 32] += float(x[k])
-        off = 1
-        while off < 32:
-            for l in range(0, 32, 2 * off):
-                lanes[l] = lanes[l] + lanes[l + off]
-            off *= 2
-        assert oracle.rsum(x) == np.float32(lanes[0])
+        assert oracle.rsum(x) == np.float32(_lane_tree(x))
+
+
+def test_rsum_of_more_than_4096_values_is_by_chunks(oracle):
+    """Beyond 4096 values: each chunk of 4096 is summed as above (in double),
+    then the chunk sums are (chunk c to lane c mod 32)."""
+    rng = np.random.default_rng(6)
+    for n in (4097, 8192, 12289, 40000, 4096 * 33 + 5):
+        x = (rng.normal(size=n) * 10.0 ** rng.integers(-3, 4, size=n)).astype(np.float32)
+        chunks = [_lane_tree(x[c:c + 4096]) for c in range(0, n, 4096)]
+        want = np.float32(_lane_tree(chunks))
+        assert oracle.rsum(x) == want
+    # and it differs from the unchunked lane sum somewhere (the definition matters)
+    x = (rng.normal(size=40000) * 10.0 ** rng.integers(-6, 7, size=40000)).astype(np.float32)
+    assert oracle.rsum(x) == np.float32(_lane_tree([_lane_tree(x[c:c + 4096]) for c in range(0, 40000, 4096)]))
