@@ -50,13 +50,17 @@ __device__ int32_t matching_contraction_map(const Team &t, Scratch &sc, char *sm
     // determine_matching_threshold (:76-86): mean of the non-negative costs
     // of the doubled edge list, CSUM over the directed list
     int64_t K = 0;
-    const double S = team_csum_count(
-        t, sc, A.n,
-        [&](int64_t e) -> double {
-            float c = A.cost[e];
-            return c >= 0.0f ? (double)c : 0.0;
-        },
-        [&](int64_t e) { return A.cost[e] >= 0.0f; }, &K);
+    const float *cost = A.cost;
+    auto nonneg = [cost](int64_t e) -> double {
+        const float c = cost[e];
+        return c >= 0.0f ? (double)c : 0.0;
+    };
+    auto counted = [cost](int64_t e) { return cost[e] >= 0.0f; };
+    double S;
+    if constexpr (std::is_same<Team, GridTeam>::value)
+        S = team_csum_count_outlined(t, sc, A.n, nonneg, counted, &K);
+    else
+        S = team_csum_count(t, sc, A.n, nonneg, counted, &K);
     int32_t prev = 0;
     if (K > 0) {
         const float sum_f = (float)(2.0 * S);

@@ -604,6 +604,18 @@ __device__ double team_csum_count(const Team &t, Scratch &sc, int64_t n, Get get
     return r;
 }
 
+// The same in a function of its own.  Inlined into the whole-GPU solve, the
+// matching threshold's sum took about 1.7x as long as called out of line
+// (the solver's live state crowds the FP64 loop).  Elsewhere (the bound of
+// message passing, the smaller teams) the call cost more than it saved, so
+// only that call site uses it.
+template <class Team, class Get, class Cnt>
+__device__ __noinline__ double team_csum_count_outlined(const Team &t, Scratch &sc, int64_t n, Get get, Cnt cnt,
+                                                        int64_t *count)
+{
+    return team_csum_count(t, sc, n, get, cnt, count);
+}
+
 template <class Team, class Get>
 __device__ double team_csum(const Team &t, Scratch &sc, int64_t n, Get get)
 {
