@@ -790,9 +790,9 @@ __device__ Csr build_symmetric_csr(const Team &t, Scratch &sc, char *sm, const G
 template <class Team>
 __device__ double graph_lb(const Team &t, Scratch &sc, const Graph &A)
 {
-    return team_csum(t, sc, A.n, [&](int64_t e) -> double {
-        float c = A.cost[e];
-        return c < 0.0f ? (double)c : 0.0;
+    return team_csum(t, sc, A.n, [&](int64_t e) -> float {
+        const float c = A.cost[e];
+        return c < 0.0f ? c : 0.0f;
     });
 }
 

@@ -24,7 +24,7 @@ __global__ void __launch_bounds__(THREADS, 2) k_objective(const int32_t *I, cons
     extern __shared__ __align__(16) char sm[];
     GridTeam t;
     Scratch sc = make_scratch(ws, bytes);
-    double s = team_csum(t, sc, n, [&](int64_t e) -> double { return lab[I[e]] != lab[J[e]] ? (double)C[e] : 0.0; });
+    double s = team_csum(t, sc, n, [&](int64_t e) -> float { return lab[I[e]] != lab[J[e]] ? C[e] : 0.0f; });
     if (t.leader()) *out = s;
 }
 

@@ -51,9 +51,9 @@ __device__ int32_t matching_contraction_map(const Team &t, Scratch &sc, char *sm
     // of the doubled edge list, CSUM over the directed list
     int64_t K = 0;
     const float *cost = A.cost;
-    auto nonneg = [cost](int64_t e) -> double {
+    auto nonneg = [cost](int64_t e) -> float {
         const float c = cost[e];
-        return c >= 0.0f ? (double)c : 0.0;
+        return c >= 0.0f ? c : 0.0f;
     };
     auto counted = [cost](int64_t e) { return cost[e] >= 0.0f; };
     double S;

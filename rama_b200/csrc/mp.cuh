@@ -292,11 +292,11 @@ __device__ __forceinline__ float tri_lb(float c12, float c13, float c23)
 template <class Team>
 __device__ double mp_lower_bound(const Team &t, Scratch &sc, const Mp &mp)
 {
-    double le = team_csum(t, sc, mp.E, [&](int64_t e) -> double {
-        float c = mp.cost[e];
-        return c < 0.0f ? (double)c : 0.0;
+    double le = team_csum(t, sc, mp.E, [&](int64_t e) -> float {
+        const float c = mp.cost[e];
+        return c < 0.0f ? c : 0.0f;
     });
-    double lt = team_csum(t, sc, mp.T, [&](int64_t k) -> double { return (double)tri_lb(mp.c12[k], mp.c13[k], mp.c23[k]); });
+    double lt = team_csum(t, sc, mp.T, [&](int64_t k) -> float { return tri_lb(mp.c12[k], mp.c13[k], mp.c23[k]); });
     return le + lt;
 }
 

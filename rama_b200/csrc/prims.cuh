@@ -544,20 +544,30 @@ __device__ double team_csum_count(const Team &t, Scratch &sc, int64_t n, Get get
             csum_t a = {0.0, 0.0};
             int64_t c = 0;
             const int64_t b0 = ch * 4096 + lane_id();
-            // 8 of the lane's 128 elements loaded at a time, merged in order
-            for (int k = 0; k < 128; k += 8) {
-                double x[8];
-                bool in[8];
+            // 8 of the lane's 128 elements loaded at a time, merged in order;
+            // the values stay as get returns them (a float takes one register)
+            // until their merge, and full chunks need no bounds checks
+            using V = decltype(get(int64_t(0)));
+            if (ch * 4096 + 4096 <= n) {
+                for (int k = 0; k < 128; k += 8) {
+                    V x[8];
 #pragma unroll
-                for (int j = 0; j < 8; ++j) {
-                    const int64_t idx = b0 + 32 * (k + j);
-                    in[j] = idx < n;
-                    x[j] = in[j] ? get(idx) : 0.0;
-                    c += in[j] && cnt(idx) ? 1 : 0;
+                    for (int j = 0; j < 8; ++j) {
+                        const int64_t idx = b0 + 32 * (k + j);
+                        x[j] = get(idx);
+                        c += cnt(idx) ? 1 : 0;
+                    }
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) a = cs_merge(a, csum_t{(double)x[j], 0.0});
                 }
-#pragma unroll
-                for (int j = 0; j < 8; ++j)
-                    if (in[j]) a = cs_merge(a, csum_t{x[j], 0.0});
+            } else {
+                for (int k = 0; k < 128; ++k) {
+                    const int64_t idx = b0 + 32 * k;
+                    if (idx < n) {
+                        a = cs_merge(a, csum_t{(double)get(idx), 0.0});
+                        c += cnt(idx) ? 1 : 0;
+                    }
+                }
             }
             a = cs_warp_tree(a);
             c = warp_sum(c);

@@ -150,7 +150,7 @@ __device__ void run_step(const Team &t, char *sm, Scratch sc, rama_step_args *a)
             a->out_nr = oom;
         }
     } else if (op == RAMA_STEP_CSUM) {
-        double s = team_csum(t, sc, a->m, [&](int64_t k) -> double { return (double)a->c[k]; });
+        double s = team_csum(t, sc, a->m, [&](int64_t k) -> float { return a->c[k]; });
         if (t.leader()) a->out_lb0 = s;
     } else if (op == RAMA_STEP_SORT) {
         uint64_t *k1 = sc.arena.take<uint64_t>(a->m + 1), *k2 = sc.arena.take<uint64_t>(a->m + 1);

@@ -296,9 +296,9 @@ __device__ bool forest_check_pentagons(const Team &t, Scratch &sc, char *sm, For
 template <class Team>
 __device__ bool forest_threshold(const Team &t, Scratch &sc, char *sm, Forest &F)
 {
-    const double S = team_csum(t, sc, F.m2, [&](int64_t k) -> double {
-        float x = F.w[k];
-        return x >= 0.0f ? (double)x : 0.0;
+    const double S = team_csum(t, sc, F.m2, [&](int64_t k) -> float {
+        const float x = F.w[k];
+        return x >= 0.0f ? x : 0.0f;
     });
     const int64_t cnt = team_sum<Team, int64_t>(t, sc, sm, F.m2, [&](int64_t k) -> int64_t { return F.w[k] >= 0.0f; });
     const float thr = (0.9f * (float)S) / (float)cnt;
