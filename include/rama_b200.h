@@ -182,10 +182,9 @@ int rama_batch_wait(rama_handle h, int64_t *num_labels, double *lbs, int32_t *st
  * pool allocator claims the device's memory should make one call (for example
  * an empty instance) before the pool reserves its memory.
  * The first call on a device also looks up the array's device address and
- * sets the kernel's shared-memory limit; make that first call before any
- * stream capture.  All calls share the one array: calls that overlap on the
- * GPU (other streams or host threads) race and must be serialised by the
- * caller.
+ * sets the kernel's shared-memory limit.  All calls share the one array:
+ * calls that overlap on the GPU (other streams or host threads) race and must
+ * be serialised by the caller.
  */
 #define RAMA_STATIC_MAX_EDGES 30000
 #define RAMA_STATIC_MAX_NODES 65536
