@@ -86,15 +86,19 @@ __device__ int64_t tri_normalize(const Team &t, Scratch &sc, char *sm, int32_t *
         int32_t *bst = sc.arena.take<int32_t>((int64_t)nmax + 2);
         int32_t *bidx = sc.arena.take<int32_t>(w + 1);
         if (sc.arena.ok() && w < (int64_t(1) << 31)) {
-            done = team_bucket_sort(
-                t, sc, sm, w, nmax + 1, [&](int64_t i) { return tlo[i]; }, [&](int64_t i) { return u1[i]; }, k2, bidx,
-                bst);
+            // the payload of each triangle is its lo, so every sorted position
+            // rebuilds its keys from its own entries
+            auto lo = [&](int64_t i) { return tlo[i]; };
+            done = team_bucket_sort_ex(
+                t, sc, sm, w, nmax + 1, lo, lo, [&](int64_t i) { return u1[i]; }, lo, k2, bidx, bst);
             if (done) {
-                for (int64_t b = t.rank(); b <= nmax; b += t.size())
-                    for (int32_t p = bst[b]; p < bst[b + 1]; ++p) {
-                        k1[p] = pack_key((int32_t)b, (int32_t)(k2[p] >> nb), nb);
-                        u2[p] = k2[p] & mask;
-                    }
+                team_for_batched(
+                    t, w, [&](int64_t p) { return make_longlong2((long long)bidx[p], (long long)k2[p]); },
+                    [&](int64_t p, longlong2 v) {
+                        const uint64_t mh = (uint64_t)v.y;
+                        k1[p] = pack_key((int32_t)v.x, (int32_t)(mh >> nb), nb);
+                        u2[p] = mh & mask;
+                    });
                 t.sync();
                 uint64_t *tp = u1;
                 u1 = u2;

@@ -147,12 +147,15 @@ __device__ bool mp_build(const Team &t, Scratch &sc, char *sm, const Graph &A, T
         int32_t *bst = sc.arena.take<int32_t>((int64_t)nmax + 2);
         bool done = false;
         if (sc.arena.ok() && nn < (int64_t(1) << 31)) {
-            done = team_bucket_sort(
-                t, sc, sm, nn, nmax + 1, [&](int64_t q) { return (int32_t)(nk1[q] >> nb); },
-                [&](int64_t q) { return nk1[q] & cmask; }, nk2, nv2, bst);
+            // the payload of each chord is its row, so every sorted position
+            // rebuilds its key from its own entries
+            auto row = [&](int64_t q) { return (int32_t)(nk1[q] >> nb); };
+            done = team_bucket_sort_ex(
+                t, sc, sm, nn, nmax + 1, row, row, [&](int64_t q) { return nk1[q] & cmask; }, row, nk2, nv2, bst);
             if (done) {
-                for (int64_t b = t.rank(); b <= nmax; b += t.size())
-                    for (int32_t p = bst[b]; p < bst[b + 1]; ++p) nk1[p] = ((uint64_t)b << nb) | nk2[p];
+                team_for_batched(
+                    t, nn, [&](int64_t p) { return ((uint64_t)(uint32_t)nv2[p] << nb) | nk2[p]; },
+                    [&](int64_t p, uint64_t key) { nk1[p] = key; });
                 t.sync();
             }
         }
