@@ -84,7 +84,9 @@ def save_cache(entry_key: str, entry: dict, path: Optional[str] = None) -> None:
     d = load_cache(path)
     d[entry_key] = entry
     os.makedirs(os.path.dirname(path) or ".", exist_ok=True)
-    tmp = path + ".tmp"
+    # one temporary per process: ranks tuning at the same time replace the
+    # file whole, never a half-written one
+    tmp = "%s.%d.tmp" % (path, os.getpid())
     with open(tmp, "w") as f:
         json.dump(d, f, indent=1, sort_keys=True)
     os.replace(tmp, path)
