@@ -64,15 +64,15 @@ def peaks():
 # so the traffic is scaled by edge count (the algorithmic bytes per edge of
 # the two sizes are close: see roofline.algorithmic_bytes).
 #   C2 (k_solve_grid), 3-D grid 64x64x32 + long range, 753,664 edges, PD:
-#     339,063,296 B read + 1,178,258,688 B written;
+#     335,417,600 B read + 1,157,507,584 B written;
 #   C4 (k_solve_mixed), 64 Delaunay graphs of the C4 generator, 1,048,829
 #     edges, PD: 407,300,096 B read + 1,957,661,440 B written.
 # Commands: ncu --metrics dram__bytes_read.sum,dram__bytes_write.sum,gpu__time_duration.sum
 #   --clock-control none -k regex:k_solve_grid -s 1 -c 1
 #   python bench.py --config c2s --steps 2 --warmup 1 --no-cpu-baseline --no-tune
 # (and -k regex:k_solve_ -s 1 -c 2 ... --config c4s --steps 3 --warmup 3 for C4)
-TRAFFIC_B_PER_EDGE = {("c2", "PD"): (339063296 + 1178258688) / 753664,
-                      ("c2s", "PD"): (339063296 + 1178258688) / 753664,
+TRAFFIC_B_PER_EDGE = {("c2", "PD"): (335417600 + 1157507584) / 753664,
+                      ("c2s", "PD"): (335417600 + 1157507584) / 753664,
                       ("c4", "PD"): (407300096 + 1957661440) / 1048829,
                       ("c4s", "PD"): (407300096 + 1957661440) / 1048829}
 
